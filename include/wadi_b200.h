@@ -1,0 +1,190 @@
+/*
+ * wadi_b200.h -- C-ABI of libwadi_b200.so, the B200 (sm_100a) form of Wadi2D's uniform-grid shallow-water step.
+ *
+ * The library drops in behind the reference's duck-typed solver backend (wadi2d/solver/backend.py:58-75, whose
+ * members are exercised by wadi2d/solver/cpu/backend.py:14-141 and wadi2d/solver/gpu/backend.py:53-203). Each entry
+ * point below names the reference member it replaces. Plain C types only: every array argument is a pointer plus a
+ * size; device pointers may come from any allocator (PyTorch tensors in the package's own host layer).
+ *
+ * Status codes (every call returns one):
+ *   W2B_OK 0, W2B_EINVAL -1 (bad argument), W2B_ECUDA -2 (a CUDA call failed), W2B_ENONFINITE -3 (a non-finite
+ *   wave speed: the reference's NumericalFailure, wadi2d/solver/stepper.py:116-118), W2B_EDTMIN -4 (the step fell
+ *   below dt_min, wadi2d/solver/stepper.py:119-123), W2B_ETIMEOUT -5 (a bounded device wait gave up).
+ *
+ * Layouts. REF_TILE is the reference's tile-with-halo state layout (wadi2d/solver/layout.py:19-50): ntiles * 1296
+ * floats, tile t, row j, column i (2-cell halo). NATIVE is this library's dense layout: the padded grid with GY guard
+ * rows and GX guard columns of zeros, pitch PX floats, cell (j, i) at (j + GY) * PX + i + GX; guards stand in for
+ * the reference's void tile. Static per-cell and per-face arrays keep the reference's (ntiles, 32, 32) tile layout;
+ * tables are repacked level-major (see w2b_pack_tables).
+ *
+ * Threading: one handle per stream; calls on one handle are not reentrant. The handle owns only host memory; every
+ * device buffer is the caller's and must outlive the handle.
+ */
+#ifndef WADI_B200_H
+#define WADI_B200_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define W2B_OK 0
+#define W2B_EINVAL (-1)
+#define W2B_ECUDA (-2)
+#define W2B_ENONFINITE (-3)
+#define W2B_EDTMIN (-4)
+#define W2B_ETIMEOUT (-5)
+
+#define W2B_LAYOUT_REF_TILE 0
+#define W2B_LAYOUT_NATIVE 1
+
+/* Field ids: the state and work arrays of wadi2d/solver/layout.py:26-30 (r is not kept: it lives in shared memory). */
+enum W2BField {
+    W2B_H = 0, W2B_D, W2B_U, W2B_V, W2B_MX, W2B_MY, W2B_QX, W2B_QY,
+    W2B_U1, W2B_V1, W2B_MX1, W2B_MY1, W2B_QX1, W2B_QY1, W2B_SRC, W2B_RES, W2B_OM, W2B_ZCX, W2B_ZCY,
+    W2B_NFIELDS
+};
+
+/* Grid of wadi2d/grid/tiles.py:19-64: ny, nx padded to multiples of 32; ntiles includes the void tile 0. */
+typedef struct {
+    int32_t ny, nx, ntiles, rows;
+} W2BGridDesc;
+
+/* The native layout of a grid, from w2b_layout. */
+typedef struct {
+    int32_t gy, gx, px;
+    int64_t ncells; /* floats per native state array: (ny + 2 gy) * px */
+} W2BLayout;
+
+/* Kernel constants: wadi2d/solver/backend.py:15-39 (NumericsRecord), plus level_fp64: the near-dry level of a cell
+ * (first table interval) inverted in FP64 instead of FP32 (off reproduces the reference's arithmetic). */
+typedef struct {
+    float g, dx, e_wet, h_cfl, u_max, lead, a_min;
+    int32_t second, sheet, mirror, carry, level_fp64;
+} W2BParams;
+
+/* Device buffers (caller-owned). Ping-pong pairs [2]: the library tracks which half is current. */
+typedef struct {
+    /* state, NATIVE layout, ncells floats each */
+    float *h[2], *u[2], *v[2], *mx[2], *my[2];
+    float *d, *qx, *qy, *qx1, *qy1, *res, *src, *om, *zcx, *zcy;
+    /* static, (ntiles, 32, 32) floats, reference tile layout */
+    const float *hc;
+    const float *fl[2], *fr[2], *gl[2], *gr[2], *ef[2], *cw[2]; /* [0] x faces, [1] y faces */
+    /* tables, level-major (w2b_pack_tables): dtab2 (ntiles, rows-1, 32, 32) float2; ftab4[a] same, float4 */
+    const float *dtab2;
+    const float *ftab4[2];
+    /* tiles: (ntiles, 2) int32 tile coordinates (tj, ti); entry 0 unused */
+    const int32_t *tiles;
+    /* (ny/32, nx/32) compact tile id of each tile position, 0 where none (wadi2d/grid/tiles.py:27-42) */
+    const int32_t *tile_of;
+    /* (ntiles, 8) neighbour tiles in the order of wadi2d/grid/tiles.py:15 */
+    const int32_t *nbr;
+    /* per-tile arrays (ntiles) */
+    int32_t *active; /* active tile list, ntiles entries */
+    float *wave;
+    int32_t *wet;
+    int32_t *keep;    /* tiles kept active whatever the water: sources and boundaries */
+    int32_t *idle;    /* checks in a row a tile was not wanted */
+    int32_t *is_act;  /* 1 on active tiles */
+    int32_t *woken;   /* tiles that joined the list at the last rebuild */
+    int32_t *scratch; /* 2 * ntiles */
+    /* (ntiles, 32) bit per cell: boundary cells, whose envelope entry follows the boundary overwrite */
+    uint32_t *bmark;
+    /* envelope, (ntiles, 32, 32) each: depth, mean depth, speed, hazard, arrival */
+    float *env[5];
+    /* control block, W2B_CTL_BYTES bytes, 256-byte aligned */
+    void *ctl;
+    /* staging for REF_TILE transfers: ntiles * 1296 floats */
+    float *stage;
+} W2BBuffers;
+
+#define W2B_CTL_BYTES 1024
+
+/* Stepper settings of wadi2d/solver/stepper.py:101-129 and the envelope cadence of wadi2d/engine/monitor.py:272-283. */
+typedef struct {
+    double cfl, wave_floor, dt_max, dt_min;
+    int32_t dt_every, active_every, adaptive; /* adaptive: sleeping tiles on */
+    int32_t max_every;                         /* envelope every this many steps, 0 = never */
+    float arrive, deep;                        /* envelope arrival and speed depths */
+} W2BStepper;
+
+/* The stepper's state, in and out of w2b_advance: the fields of wadi2d/solver/stepper.py:24-47. */
+typedef struct {
+    double t, dt;
+    int64_t nsteps;
+    int32_t refresh_due;
+    int32_t status;
+    float wave_max;
+    int32_t nact;
+} W2BClock;
+
+int32_t w2b_version(void);
+
+/* Native layout of a grid. */
+int32_t w2b_layout(const W2BGridDesc* grid, W2BLayout* out);
+
+/* Native index of reference state indices (host arrays; halo entries map to the neighbour cell they copy). */
+int32_t w2b_ref_to_native(const W2BGridDesc* grid, const int32_t* tiles_host, int64_t n, const int64_t* ref_index,
+                          int64_t* native_index);
+
+/* Replaces GpuBackend.__init__ (wadi2d/solver/gpu/backend.py:58-104): binds the buffers; allocates nothing on the
+ * device. The caller has zeroed the state buffers and filled the static ones. */
+int32_t w2b_create(const W2BGridDesc* grid, const W2BParams* params, const W2BBuffers* buffers, void** handle);
+int32_t w2b_destroy(void* handle);
+
+/* Replace the kernel constants (a new cell size or switch); the next device loop recaptures its graphs. */
+int32_t w2b_set_params(void* handle, const W2BParams* params);
+
+/* Repack reference tables (device, (ntiles,32,32,rows) and (ntiles,32,32,rows,2)) into the level-major pairs. */
+int32_t w2b_pack_tables(const W2BGridDesc* grid, const float* dtab, const float* ftabx, const float* ftaby,
+                        float* dtab2, float* ftab4x, float* ftab4y, void* stream);
+
+/* Replaces set_active (wadi2d/solver/gpu/backend.py:116-119): tiles is a device array of n tile ids. */
+int32_t w2b_set_active(void* handle, const int32_t* tiles, int32_t n, void* stream);
+
+/* Replaces set_boundary (wadi2d/solver/gpu/backend.py:127-132). Device arrays of n entries; cell and ref are NATIVE
+ * indices (w2b_ref_to_native). kind 0 fixed (h0, d0), 1 free, 2 follows ref lowered by d0. */
+int32_t w2b_set_boundary(void* handle, int32_t n, const int32_t* cell, const int32_t* ref, const int32_t* kind,
+                         const float* d0, const float* h0);
+
+/* The boundary tally of wadi2d/engine/maxima.py:149-192: n faces (NATIVE index, axis 0 x / 1 y, sign), one FP64
+ * total per face in total[n]. Device arrays. */
+int32_t w2b_set_tally(void* handle, int32_t n, const int32_t* face, const int32_t* axis, const float* sign,
+                      double* total);
+
+/* Replaces step (wadi2d/solver/gpu/backend.py:151-188): faces, positivity, update, boundary, then the swap. */
+int32_t w2b_step(void* handle, float dt, int32_t want_wave, int32_t want_wet, void* stream);
+
+/* Replaces max_wave / wet_flags (wadi2d/solver/gpu/backend.py:196-200): copy to host, synchronising the stream. */
+int32_t w2b_max_wave(void* handle, float* out, void* stream);
+int32_t w2b_wet_flags(void* handle, int32_t* out, void* stream);
+
+/* Replaces refresh_plan (wadi2d/solver/gpu/backend.py:139-143): tiles is a device array. */
+int32_t w2b_refresh_plan(void* handle, const int32_t* tiles, int32_t n, void* stream);
+
+/* Current device pointer of a field (ping-pong pairs resolve to their current half). */
+int32_t w2b_field_ptr(void* handle, int32_t field, float** out);
+
+/* Replaces get_field / set_field (wadi2d/solver/gpu/backend.py:121-125). layout REF_TILE or NATIVE; host != 0 means
+ * the other pointer is host memory (pinned for an asynchronous copy). REF_TILE writes own cells only: halo entries
+ * of the reference layout are copies and are read back from their owners. */
+int32_t w2b_get_field(void* handle, int32_t field, float* dst, int32_t layout, int32_t host, void* stream);
+int32_t w2b_set_field(void* handle, int32_t field, const float* src, int32_t layout, int32_t host, void* stream);
+
+/* Replaces Maxima.update (wadi2d/engine/maxima.py:118-130) over the active tiles, and Tally.add (:171-182). */
+int32_t w2b_maxima(void* handle, float t, float arrive, float deep, void* stream);
+int32_t w2b_tally(void* handle, double dt, void* stream);
+
+/* Replaces the loop of Stepper.advance (wadi2d/solver/stepper.py:101-129) with a device-resident one: steps until
+ * clock->t reaches t_end or max_steps steps ran, the step rule, refresh cadence, sleeping tiles, the envelope every
+ * max_every steps and the boundary tally every step all on the device. clock is read and written (host memory). */
+int32_t w2b_advance(void* handle, const W2BStepper* cfg, double t_end, int64_t max_steps, W2BClock* clock,
+                    void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

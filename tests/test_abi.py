@@ -1,0 +1,64 @@
+"""The C-ABI library loads and exports every entry point include/wadi_b200.h declares; the host-only entry points
+(layout and index conversion) agree with the Python layout helpers. No GPU needed."""
+
+from __future__ import annotations
+
+import ctypes
+import re
+from pathlib import Path
+
+import numpy as np
+
+from wadi2d_b200 import _lib, build, layout
+from wadi2d_b200.grid import TileGrid
+
+HEADERS = sorted((Path(__file__).resolve().parents[1] / "include").glob("*.h"))
+
+
+def declared() -> list[str]:
+    names = []
+    for h in HEADERS:
+        names += re.findall(r"^\s*int32_t\s+(w2b_\w+)\s*\(", h.read_text(), flags=re.M)
+    return sorted(set(names))
+
+
+def test_library_exports_every_declared_symbol():
+    build.build()
+    lib = _lib.lib()
+    names = declared()
+    assert len(names) >= 20
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+    assert set(names) <= set(_lib._SIGNATURES) | {n for n in names if n.startswith("w2b_")}
+
+
+def test_every_bound_signature_is_declared():
+    assert set(_lib._SIGNATURES) <= set(declared())
+
+
+def test_layout_and_index_conversion_match_python():
+    rng = np.random.default_rng(0)
+    mask = rng.random((70, 90)) > 0.3
+    g = TileGrid.from_mask(mask, 0.0, 0.0, 10.0)
+    desc = _lib.GridDesc(g.shape[0], g.shape[1], g.ntiles, 16)
+    lay = _lib.Layout()
+    assert _lib.lib().w2b_layout(ctypes.byref(desc), ctypes.byref(lay)) == 0
+    assert lay.px == layout.native_pitch(g.shape[1])
+    assert lay.ncells == layout.native_size(*g.shape)
+    ref = rng.integers(layout.STRIDE2, g.ntiles * layout.STRIDE2, 5000).astype(np.int64)
+    out = np.zeros_like(ref)
+    tiles = np.ascontiguousarray(g.tiles, np.int32)
+    st = _lib.lib().w2b_ref_to_native(ctypes.byref(desc), tiles.ctypes.data, ref.size, ref.ctypes.data,
+                                      out.ctypes.data)  # fmt: skip
+    assert st == 0
+    assert np.array_equal(out, layout.native_of_ref(g.tiles, ref, g.shape[1]))
+
+
+def test_bad_arguments_are_refused_without_a_gpu():
+    bad = _lib.GridDesc(33, 64, 2, 16)
+    assert _lib.lib().w2b_layout(ctypes.byref(bad), ctypes.byref(_lib.Layout())) == _lib.EINVAL
+    g = _lib.GridDesc(64, 64, 2, 16)
+    tiles = np.array([[-1, -1], [0, 0]], np.int32)
+    ref = np.array([5], np.int64)  # an entry of the void tile
+    out = np.zeros(1, np.int64)
+    assert _lib.lib().w2b_ref_to_native(ctypes.byref(g), tiles.ctypes.data, 1, ref.ctypes.data, out.ctypes.data) == -1

@@ -1,0 +1,197 @@
+// Shared device definitions of libwadi_b200: layout constants, the control block, the argument records, and the
+// float32 helpers of the step. The helpers restate wadi2d/solver/gpu/kernels/common.cuh:22-96 (= the Numba twin
+// wadi2d/solver/cpu/kernels.py:19-83) in the same statement order; the library is compiled with -fmad=false and
+// IEEE division and square root, so with identical inputs each helper returns the reference CPU twin's bits.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "wadi_b200.h"
+
+namespace w2b {
+
+constexpr int TILE = 32;
+constexpr int TILE2 = TILE * TILE;
+constexpr int GY = 4;   // guard rows above and below the padded grid in the native layout
+constexpr int GX = 32;  // guard columns left and right: keeps every tile row 128-byte aligned
+constexpr int SLEEP_CHECKS = 2;  // wadi2d/solver/stepper.py:12
+
+// Device control block, W2B_CTL_BYTES long. Written by the host's set-step kernel or by the device loop's control
+// kernel, read by every step kernel.
+struct Ctl {
+    // this step
+    float dtf;          // dt as the kernels take it, float32
+    int32_t run;        // 0: the device loop has finished, kernels return at once
+    int32_t want_wave;  // refresh step: wave speeds and the wet share om
+    int32_t want_wet;   // active-list step: tile wet flags
+    int32_t want_max;   // envelope step
+    float max_time;     // envelope time (float32 of t after the step)
+    double dt_tally;    // t after the step minus t before it, FP64
+    double dt_step;     // this step's dt, FP64 (the device loop)
+    int32_t nact;       // active tiles
+    uint32_t ticket;    // last-block counter of the wave reduction
+    float wave_max;     // max wave over active tiles of the last refresh step
+    int32_t activate;   // this step rebuilds the active list (device loop)
+    // device loop clock (wadi2d/solver/stepper.py:24-47)
+    double t, dt, t_end;
+    long long nsteps, steps_run, max_steps;
+    int32_t refresh_due, status;
+    int32_t nwoken;
+    int32_t pad0;
+    // stepper settings
+    double cfl, wave_floor, dt_max, dt_min, dx;
+    int32_t dt_every, active_every, adaptive, max_every;
+    float arrive, deep;
+};
+static_assert(sizeof(Ctl) <= W2B_CTL_BYTES, "control block too large");
+
+// Everything a step kernel reads, with the ping-pong halves resolved for one parity.
+struct StepArgs {
+    W2BParams P;
+    int32_t rows, px, ntiles, nty, ntx;
+    float area;  // dx * dx
+    // state, native
+    const float* __restrict__ h;  // current mean depth
+    float* __restrict__ h_next;
+    const float* __restrict__ u[2];  // current face velocities, x then y
+    float* __restrict__ u_next[2];
+    const float* __restrict__ m[2];  // current face momenta
+    float* __restrict__ m_next[2];
+    float* __restrict__ d;
+    float* __restrict__ q[2];   // qx, qy: scaled discharges
+    float* __restrict__ q1[2];  // qx1, qy1: unscaled, from the face pass
+    float* __restrict__ res;
+    const float* __restrict__ src;
+    float* __restrict__ om;
+    const float* __restrict__ zc[2];
+    // static, tile layout
+    const float* __restrict__ hc;
+    const float* __restrict__ fl[2];
+    const float* __restrict__ fr[2];
+    const float* __restrict__ gl[2];
+    const float* __restrict__ gr[2];
+    const float* __restrict__ ef[2];
+    const float* __restrict__ cw[2];
+    const float2* __restrict__ dtab2;
+    const float4* __restrict__ ftab4[2];
+    const int32_t* __restrict__ tiles;
+    const int32_t* __restrict__ tile_of;
+    const int32_t* __restrict__ nbr;
+    int32_t* __restrict__ active;
+    float* __restrict__ wave;
+    int32_t* __restrict__ wet;
+    int32_t* __restrict__ keep;
+    int32_t* __restrict__ idle;
+    int32_t* __restrict__ is_act;
+    int32_t* __restrict__ woken;
+    int32_t* __restrict__ scratch;
+    float* __restrict__ env[5];
+    const uint32_t* __restrict__ bmark;
+    // boundary cells and tally faces
+    int32_t nb;
+    const int32_t* __restrict__ bcell;
+    const int32_t* __restrict__ bref;
+    const int32_t* __restrict__ bkind;
+    const float* __restrict__ bd0;
+    const float* __restrict__ bh0;
+    int32_t ntally;
+    const int32_t* __restrict__ tface;
+    const int32_t* __restrict__ taxis;
+    const float* __restrict__ tsign;
+    double* __restrict__ ttotal;
+    Ctl* ctl;
+};
+
+// ------------------------------------------------------------------ float32 helpers
+
+// Numba's float32 cbrt is float(cbrt(double(x))); this is the same composition with CUDA's double cbrt.
+__device__ __forceinline__ float cbrt32(float x) { return (float)cbrt((double)x); }
+// Python max/min on two ordered floats (the first argument wins a tie).
+__device__ __forceinline__ float fmax32(float a, float b) { return a >= b ? a : b; }
+__device__ __forceinline__ float fmin32(float a, float b) { return a <= b ? a : b; }
+
+__device__ __forceinline__ float minmod(float a, float b) {
+    if (a * b <= 0.0f) return 0.0f;
+    return fabsf(a) < fabsf(b) ? a : b;
+}
+
+__device__ __forceinline__ float ustar(float uc, float uup, float udown, int second) {
+    if (!second) return uc;
+    return uc + 0.5f * minmod(uc - uup, udown - uc);
+}
+
+__device__ __forceinline__ float gated(float neighbour, float own, int mirror) {
+    return (mirror && neighbour == 0.0f) ? own : neighbour;
+}
+
+__device__ __forceinline__ bool not_finite(float v) { return (__float_as_int(v) & 0x7f800000) == 0x7f800000; }
+
+// Row index of a quadratic table, clamped to [0, last - 1] so that no input can read outside the table.
+__device__ __forceinline__ int row_of(float s, int last) {
+    int r = (int)s;
+    r = r < 0 ? 0 : r;
+    return r > last - 1 ? last - 1 : r;
+}
+
+// Level above zmin from mean depth, wadi2d/solver/gpu/kernels/common.cuh:39-47. pair(r) = (tab[r], tab[r + 1]).
+__device__ __forceinline__ float cell_level(float hb, float hc, const float2* __restrict__ pairs, int rows,
+                                            int fp64) {
+    if (hc <= 0.0f) return hb;
+    const int last = rows - 1;
+    if (hb >= hc) {
+        const float2 p = __ldg(pairs + (size_t)(last - 1) * TILE2);
+        return p.y + (hb - hc);
+    }
+    const float s = sqrtf(hb / hc) * (float)last;
+    const int r = row_of(s, last);
+    const float2 p = __ldg(pairs + (size_t)r * TILE2);
+    if (fp64 && r == 0) {
+        // near-dry bottom interval: the row coordinate and the interpolation in FP64
+        const double sd = sqrt((double)hb / (double)hc) * (double)last;
+        return (float)((double)p.x + sd * ((double)p.y - (double)p.x));
+    }
+    return p.x + (s - (float)r) * (p.y - p.x);
+}
+
+// Wet share of the cell plan, wadi2d/solver/gpu/kernels/common.cuh:49-57.
+__device__ __forceinline__ float cell_plan(float hb, float hc, const float2* __restrict__ pairs, int rows) {
+    if (hc <= 0.0f || hb >= hc) return 1.0f;
+    const int last = rows - 1;
+    const float s = sqrtf(hb / hc) * (float)last;
+    const int r = row_of(s, last);
+    const float m = (float)last;
+    const float2 p = __ldg(pairs + (size_t)r * TILE2);
+    return hc * (float)(2 * r + 1) / (m * m) / fmax32(p.y - p.x, 1e-12f);
+}
+
+// Area, conveyance^(3/5) and wet width at depth e over the face invert, wadi2d/solver/gpu/kernels/common.cuh:64-91.
+// quad(r) = (A_r, T_r, A_r+1, T_r+1).
+__device__ __forceinline__ void face_lookup(float e, float top, const float4* __restrict__ quads, int rows, float& A,
+                                            float& T, float& W) {
+    const int last = rows - 1;
+    const float m = (float)last;
+    if (e >= top) {
+        const float4 q = __ldg(quads + (size_t)(last - 1) * TILE2);
+        const float a1 = q.z;
+        const float a0 = q.x;
+        const float c = (m - 1.0f) / m;
+        W = (a1 - a0) / (top * (1.0f - c * c));
+        A = a1 + W * (e - top);
+        T = q.w * (A / fmax32(a1, 1e-12f));
+        return;
+    }
+    const float s = sqrtf(e / top) * m;
+    const int r = row_of(s, last);
+    const float c0 = (float)r / m;
+    const float c1 = (float)(r + 1) / m;
+    const float e0 = c0 * c0 * top;
+    const float de = (c1 * c1 - c0 * c0) * top;
+    const float f = (e - e0) / de;
+    const float4 q = __ldg(quads + (size_t)r * TILE2);
+    A = q.x + f * (q.z - q.x);
+    T = q.y + f * (q.w - q.y);
+    W = (q.z - q.x) / de;
+}
+
+}  // namespace w2b

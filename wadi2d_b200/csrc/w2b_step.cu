@@ -1,0 +1,619 @@
+// The uniform-grid step on sm_100a: face pass, update pass (positivity ratio, continuity, level lookup, envelope),
+// boundary/tally/control pass, active-list rebuild, and the layout converters.
+//
+// One CTA of 256 threads (32 x 8) takes one 32 x 32 tile at a time, looping over the active list (grid-stride, so a
+// graph-captured launch serves any list length). Each thread owns one column and four rows of the tile. State sits
+// in the dense NATIVE layout, so a neighbour is an address offset and the reference's halo exchanges
+// (wadi2d/solver/gpu/kernels/cells.cu:80-93) disappear; the guard ring is zero like the reference's void tile.
+//
+// The face pass restates wadi2d/solver/gpu/kernels/faces.cu:10-175 (= wadi2d/solver/cpu/kernels.py:86-244); the
+// update pass fuses limit and update (cells.cu:4-63, kernels.py:247-299) by computing the positivity ratio r of the
+// tile and its one-cell ring in shared memory; the boundary pass restates cells.cu:95-111 and engine/maxima.py:53-62.
+#include <cstdio>
+
+#include "w2b_common.cuh"
+
+namespace w2b {
+
+// ------------------------------------------------------------------ face pass
+
+// One face: AX 0 is the west (x) face of cell k, AX 1 its north (y) face. Returns the wave speed.
+template <int AX>
+__device__ __forceinline__ float face_step(const StepArgs& A, int k, int fid, int t, int local, float dt,
+                                           int want_wave) {
+    const W2BParams& P = A.P;
+    const int s = AX == 0 ? 1 : A.px;  // along the normal
+    const int p = AX == 0 ? A.px : 1;  // across it
+    const float* __restrict__ u = A.u[AX];
+    const float* __restrict__ m = A.m[AX];
+    const float* __restrict__ q = A.q[AX];
+    const float* __restrict__ qp = A.q[1 - AX];
+    const float* __restrict__ vp = A.u[1 - AX];
+    const float* __restrict__ d = A.d;
+    const float* __restrict__ h = A.h;
+    const float ZERO = 0.0f, HALF = 0.5f, ONE = 1.0f;
+    const float dx = P.dx;
+    const float span = dx;
+
+    const float fl = __ldg(A.fl[AX] + fid);
+    const float fr = __ldg(A.fr[AX] + fid);
+    const float e_l = __ldg(d + k - s) - fl;
+    const float e_r = __ldg(d + k) - fr;
+    const float uf = __ldg(u + k);
+    const float e_lp = fmax32(e_l, ZERO);
+    const float e_rp = fmax32(e_r, ZERO);
+    const bool from_left = uf > ZERO || (uf == ZERO && e_l >= e_r);
+    const float eup = from_left ? e_lp : e_rp;
+    if (eup <= P.e_wet) {
+        A.u_next[AX][k] = ZERO;
+        A.m_next[AX][k] = ZERO;
+        A.q1[AX][k] = ZERO;
+        return ZERO;
+    }
+    const float cwf = __ldg(A.cw[AX] + fid);
+    const float top = __ldg(A.ef[AX] + fid);
+    float eface = eup;
+    if (P.carry && cwf == ZERO) {
+        const float dz = from_left ? __ldg(A.zc[AX] + k - s) - fl : __ldg(A.zc[AX] + k) - fr;
+        if (dz > 1e-6f) {
+            float phi = (eup - 2.0f * dz) / (2.0f * dz);
+            phi = phi < ZERO ? ZERO : (phi > ONE ? ONE : phi);
+            eface = eup - phi * dz;
+        }
+    }
+    const float4* __restrict__ quads = A.ftab4[AX] + (size_t)t * (A.rows - 1) * TILE2 + local;
+    float area, tt, w;
+    face_lookup(eface, top, quads, A.rows, area, tt, w);
+    const float h_l = __ldg(h + k - s);
+    const float h_r = __ldg(h + k);
+    const float hup = from_left ? h_l : h_r;
+
+    // [1] section
+    float rho = ONE;
+    float d_eta = e_rp - e_lp;
+    if (P.sheet) {
+        const float avol = hup * dx;
+        const float edown = from_left ? e_rp : e_lp;
+        if (avol < area) {
+            const float sub = fmin32(e_lp, e_rp) / fmax32(e_lp, e_rp);
+            const float sub2 = sub * sub;
+            const float alpha = sub2 * sub2;
+            rho = alpha + (ONE - alpha) * avol / area;
+        }
+        if (edown <= ZERO) {
+            // [2] disconnected
+            const float g_u = from_left ? __ldg(A.gl[AX] + fid) : __ldg(A.gr[AX] + fid);
+            const float g_d = from_left ? __ldg(A.gr[AX] + fid) : __ldg(A.gl[AX] + fid);
+            const float h_d = from_left ? h_r : h_l;
+            const float drop = (hup - g_u) - fmax32(h_d - g_d, HALF * (g_u - g_d));
+            const float level_drop = fabsf(e_l - e_r);
+            const float drive = fmax32(eup, fmin32(drop, level_drop));
+            d_eta = from_left ? -drive : drive;
+        }
+    }
+
+    // [3] momentum fluxes
+    const int mirror = P.mirror, second = P.second;
+    const float um = gated(__ldg(u + k - s), uf, mirror);
+    const float up = gated(__ldg(u + k + s), uf, mirror);
+    const float umm = gated(__ldg(u + k - 2 * s), um, mirror);
+    const float upp = gated(__ldg(u + k + 2 * s), up, mirror);
+    const float qk = __ldg(q + k);
+    const float qc_l = HALF * (__ldg(q + k - s) + qk);
+    const float qc_r = HALF * (qk + __ldg(q + k + s));
+    const float s_l = qc_l > ZERO ? ustar(um, umm, uf, second) : ustar(uf, up, um, second);
+    const float s_r = qc_r > ZERO ? ustar(uf, um, up, second) : ustar(up, upp, uf, second);
+    float flux = qc_r * s_r - qc_l * s_l;
+    const float qy_s = HALF * (__ldg(qp + k - s) + __ldg(qp + k));
+    const float qy_n = HALF * (__ldg(qp + k - s + p) + __ldg(qp + k + p));
+    const float u_s = gated(__ldg(u + k - p), uf, mirror);
+    const float u_n = gated(__ldg(u + k + p), uf, mirror);
+    const float uss = gated(__ldg(u + k - 2 * p), u_s, mirror);
+    const float unn = gated(__ldg(u + k + 2 * p), u_n, mirror);
+    const float us_s = qy_s > ZERO ? ustar(u_s, uss, uf, second) : ustar(uf, u_n, u_s, second);
+    const float us_n = qy_n > ZERO ? ustar(uf, u_s, u_n, second) : ustar(u_n, unn, uf, second);
+    flux += qy_n * us_n - qy_s * us_s;
+
+    // [4] momentum and pressure
+    const float abar = HALF * (h_l + h_r) * dx;
+    const float press = dt * P.g * d_eta / span;
+    float us;
+    if (abar > 1e-6f * dx)
+        us = (__ldg(m + k) - dt * flux / span) / abar - press;
+    else
+        us = uf - press;
+
+    // [5] friction
+    const float vb = 0.25f * (__ldg(vp + k - s) + __ldg(vp + k) + __ldg(vp + k - s + p) + __ldg(vp + k + p));
+    const float t3 = tt * tt * tt * cbrt32(tt);
+    float fric = area * area / fmax32(t3, 1e-30f);
+    if (rho < ONE) fric = fric / fmax32(rho * cbrt32(rho), 1e-12f);
+    const float a = dt * P.g * fric;
+    const float sp = sqrtf(us * us + vb * vb);
+    float un = 2.0f * us / (ONE + sqrtf(ONE + 4.0f * a * sp));
+    if (fabsf(un) > P.u_max) un = un > ZERO ? P.u_max : -P.u_max;
+
+    // [6] crest face
+    float qn = area * rho * un;
+    float c = cwf;
+    if (c != ZERO) {
+        float area_c = area, w_c = w;
+        if (c < ZERO) {
+            c = -c;
+            const float ua = from_left ? um : up;
+            float tc;
+            face_lookup(eup + HALF * ua * ua / P.g, top, quads, A.rows, area_c, tc, w_c);
+        }
+        const float qc = c * area_c * sqrtf(area_c / fmax32(w_c, 1e-9f));
+        if (fabsf(qn) > qc) {
+            qn = qn > ZERO ? qc : -qc;
+            un = qn / fmax32(area * rho, 1e-12f);
+        }
+    }
+    A.u_next[AX][k] = un;
+    A.m_next[AX][k] = abar * un;
+    A.q1[AX][k] = qn;
+    if (!want_wave) return ZERO;
+    if (not_finite(un)) return 1e30f;
+    const float d_left = __ldg(d + k - s);
+    const float d_right = __ldg(d + k);
+    const float dup = from_left ? d_left : d_right;
+    if (dup <= P.h_cfl) return ZERO;
+    float plan = from_left ? __ldg(A.om + k - s) : __ldg(A.om + k);
+    const float dother = from_left ? d_right : d_left;
+    if (dother > P.h_cfl) plan = fmin32(plan, from_left ? __ldg(A.om + k) : __ldg(A.om + k - s));
+    const float wave = sqrtf(fmax32(P.g * area * rho / (fmax32(plan, P.a_min) * dx), ZERO));
+    return fabsf(un) + fmin32(P.lead * fabsf(un - uf), 2.0f * wave) + wave;
+}
+
+__device__ __forceinline__ float warp_max(float v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax32(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+
+// Block-wide max of v (256 threads); the result is valid in thread 0.
+__device__ __forceinline__ float block_max(float v, float* red) {
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    v = warp_max(v);
+    if ((tid & 31) == 0) red[tid >> 5] = v;
+    __syncthreads();
+    float r = 0.0f;
+    if (tid < 32) {
+        r = tid < (int)(blockDim.x * blockDim.y) / 32 ? red[tid] : 0.0f;
+        r = warp_max(r);
+    }
+    __syncthreads();
+    return r;
+}
+
+__global__ void __launch_bounds__(256) faces_kernel(StepArgs A) {
+    Ctl* ctl = A.ctl;
+    if (!ctl->run) return;
+    const int nact = ctl->nact;
+    const float dt = ctl->dtf;
+    const int want_wave = ctl->want_wave;
+    __shared__ float red[8];
+    for (int a = blockIdx.x; a < nact; a += gridDim.x) {
+        const int t = A.active[a];
+        const int tj = A.tiles[2 * t], ti = A.tiles[2 * t + 1];
+        const int base = (tj * TILE + GY) * A.px + ti * TILE + GX;
+        float wmax = 0.0f;
+#pragma unroll 1
+        for (int c = 0; c < 4; ++c) {
+            const int jj = threadIdx.y * 4 + c;
+            const int ii = threadIdx.x;
+            const int k = base + jj * A.px + ii;
+            const int local = jj * TILE + ii;
+            const int fid = t * TILE2 + local;
+            const float wx = face_step<0>(A, k, fid, t, local, dt, want_wave);
+            const float wy = face_step<1>(A, k, fid, t, local, dt, want_wave);
+            wmax = fmax32(wmax, fmax32(wx, wy));
+        }
+        if (want_wave) {
+            const float bm = block_max(wmax, red);
+            if (threadIdx.x == 0 && threadIdx.y == 0) A.wave[t] = bm;
+        }
+    }
+    if (!want_wave) return;
+    // single-pass grid reduction: the last CTA to finish reduces the per-tile maxima (no CTA waits on another)
+    __shared__ bool last;
+    if (threadIdx.x == 0 && threadIdx.y == 0) {
+        __threadfence();
+        const unsigned v = atomicAdd(&ctl->ticket, 1u);
+        last = (v == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    float w = 0.0f;
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    for (int a = tid; a < nact; a += blockDim.x * blockDim.y) w = fmax32(w, __ldcg(A.wave + A.active[a]));
+    const float bm = block_max(w, red);
+    if (tid == 0) {
+        ctl->wave_max = bm;
+        ctl->ticket = 0u;
+    }
+}
+
+// ------------------------------------------------------------------ update pass
+
+__device__ __forceinline__ float scaled(float q, float rl, float rr) { return q * (q > 0.0f ? rl : rr); }
+
+// Envelope of one own cell, wadi2d/engine/maxima.py:75-92 (the CPU twin forms the centre speed in float64).
+__device__ __forceinline__ void envelope(const StepArgs& A, int fid, int k, float dk, float hk, float time,
+                                         float arrive, float deep) {
+    float* __restrict__ dmax = A.env[0];
+    float* __restrict__ hmax = A.env[1];
+    float* __restrict__ smax = A.env[2];
+    float* __restrict__ zmax = A.env[3];
+    float* __restrict__ tarr = A.env[4];
+    dmax[fid] = fmax32(dmax[fid], dk);
+    hmax[fid] = fmax32(hmax[fid], hk);
+    if (dk > deep) {
+        const double uc = 0.5 * (double)(A.u_next[0][k] + A.u_next[0][k + 1]);
+        const double vc = 0.5 * (double)(A.u_next[1][k] + A.u_next[1][k + A.px]);
+        const double s = sqrt(uc * uc + vc * vc);
+        const double sm = (double)smax[fid];
+        smax[fid] = (float)(sm >= s ? sm : s);
+        const double hz = s * (double)dk;
+        const double zm = (double)zmax[fid];
+        zmax[fid] = (float)(zm >= hz ? zm : hz);
+    }
+    if (tarr[fid] < 0.0f && dk >= arrive) tarr[fid] = time;
+}
+
+constexpr int RING = TILE + 2;  // the tile and its one-cell ring
+constexpr int RPAD = RING + 1;
+
+__global__ void __launch_bounds__(256) update_kernel(StepArgs A) {
+    Ctl* ctl = A.ctl;
+    if (!ctl->run) return;
+    const int nact = ctl->nact;
+    const float dt = ctl->dtf;
+    const int want_plan = ctl->want_wave;
+    const int want_wet = ctl->want_wet;
+    const int want_max = ctl->want_max;
+    const float time = ctl->max_time, arrive = ctl->arrive, deep = ctl->deep;
+    const float area = A.area;
+    const int px = A.px;
+    const float* __restrict__ q1x = A.q1[0];
+    const float* __restrict__ q1y = A.q1[1];
+    __shared__ float rs[RING * RPAD];
+    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    for (int a = blockIdx.x; a < nact; a += gridDim.x) {
+        const int t = A.active[a];
+        const int tj = A.tiles[2 * t], ti = A.tiles[2 * t + 1];
+        const int base = (tj * TILE + GY) * px + ti * TILE + GX;
+        // positivity ratio r of the tile and its ring (wadi2d/solver/gpu/kernels/cells.cu:4-19), from the old h
+        for (int idx = tid; idx < RING * RING; idx += 256) {
+            const int rj = idx / RING, ri = idx - rj * RING;
+            const int k = base + (rj - 1) * px + (ri - 1);
+            const float out = fmax32(__ldg(q1x + k + 1), 0.0f) + fmax32(-__ldg(q1x + k), 0.0f) +
+                              fmax32(__ldg(q1y + k + px), 0.0f) + fmax32(-__ldg(q1y + k), 0.0f);
+            const float have = fmax32(__ldg(A.h + k), 0.0f) * area;
+            rs[rj * RPAD + ri] = out * dt > have ? have / (out * dt) : 1.0f;
+        }
+        __syncthreads();
+        int any = 0;
+        const float2* __restrict__ pairs_t = A.dtab2 + (size_t)t * (A.rows - 1) * TILE2;
+#pragma unroll 1
+        for (int c = 0; c < 4; ++c) {
+            const int jj = threadIdx.y * 4 + c;
+            const int ii = threadIdx.x;
+            const int k = base + jj * px + ii;
+            const int local = jj * TILE + ii;
+            const int fid = t * TILE2 + local;
+            const float* row = rs + (jj + 1) * RPAD + (ii + 1);
+            const float rc = row[0];
+            const float qw = scaled(__ldg(q1x + k), row[-1], rc);
+            const float qe = scaled(__ldg(q1x + k + 1), rc, row[1]);
+            const float qn = scaled(__ldg(q1y + k), row[-RPAD], rc);
+            const float qs = scaled(__ldg(q1y + k + px), rc, row[RPAD]);
+            A.q[0][k] = qw;
+            A.q[1][k] = qn;
+            const float h0 = __ldg(A.h + k);
+            const float inc = A.res[k] + dt * __ldg(A.src + k) - dt * (qe - qw + qs - qn) / area;
+            const float total = h0 + inc;
+            const float hn = fmax32(total, 0.0f);
+            A.res[k] = total > 0.0f ? inc - (total - h0) : 0.0f;
+            A.h_next[k] = hn;
+            const float hcv = __ldg(A.hc + fid);
+            const float dk = cell_level(hn, hcv, pairs_t + local, A.rows, A.P.level_fp64);
+            A.d[k] = dk;
+            if (want_plan) A.om[k] = cell_plan(hn, hcv, pairs_t + local, A.rows);
+            any |= hn > 0.0f;
+            if (want_max && !((A.bmark[t * TILE + jj] >> ii) & 1u)) envelope(A, fid, k, dk, hn, time, arrive, deep);
+        }
+        if (want_wet) {
+            const int w = __syncthreads_or(any);
+            if (tid == 0) A.wet[t] = w;
+        } else {
+            __syncthreads();
+        }
+    }
+}
+
+// ------------------------------------------------------------------ boundary, tally, control (one CTA)
+
+__device__ __forceinline__ int fid_of_native(const StepArgs& A, int k) {
+    const int j = k / A.px - GY;
+    const int i = k - (j + GY) * A.px - GX;
+    const int t = A.tile_of[(j / TILE) * A.ntx + (i / TILE)];
+    return t * TILE2 + (j % TILE) * TILE + (i % TILE);
+}
+
+__global__ void boundary_kernel(StepArgs A, int control) {
+    Ctl* ctl = A.ctl;
+    if (!ctl->run) return;
+    const int tid = threadIdx.x;
+    for (int m = tid; m < A.nb; m += blockDim.x) {
+        const int k = A.bcell[m];
+        const int kind = A.bkind[m];
+        if (kind == 0) {
+            A.h_next[k] = A.bh0[m];
+            A.d[k] = A.bd0[m];
+        } else if (kind == 1) {
+            A.h_next[k] = 0.0f;
+            A.d[k] = 0.0f;
+        } else {
+            const int r = A.bref[m];
+            A.h_next[k] = A.h_next[r];
+            A.d[k] = fmax32(A.d[r] + A.bd0[m], 0.0f);
+        }
+    }
+    __syncthreads();
+    if (ctl->want_max) {
+        for (int m = tid; m < A.nb; m += blockDim.x) {
+            const int k = A.bcell[m];
+            envelope(A, fid_of_native(A, k), k, A.d[k], A.h_next[k], ctl->max_time, ctl->arrive, ctl->deep);
+        }
+    }
+    if (control) {
+        const double dtt = ctl->dt_tally;
+        for (int m = tid; m < A.ntally; m += blockDim.x) {
+            const float qv = A.taxis[m] ? A.q[1][A.tface[m]] : A.q[0][A.tface[m]];
+            A.ttotal[m] += dtt * (double)(A.tsign[m] * qv);
+        }
+    }
+    if (!control) return;
+    __syncthreads();
+    if (tid != 0) return;
+    // the stepper's bookkeeping after a step, wadi2d/solver/stepper.py:113-124
+    ctl->t = ctl->t + ctl->dt_step;
+    ctl->nsteps += 1;
+    ctl->steps_run += 1;
+    if (ctl->want_wave) {
+        const double w = (double)ctl->wave_max;
+        if (!isfinite(w)) {
+            ctl->status = W2B_ENONFINITE;
+        } else {
+            const double lim = ctl->cfl * ctl->dx / (ctl->wave_floor > w ? ctl->wave_floor : w);
+            ctl->dt = ctl->dt_max < lim ? ctl->dt_max : lim;
+            if (ctl->dt < ctl->dt_min) ctl->status = W2B_EDTMIN;
+        }
+    }
+}
+
+// Before a step of the device loop: the loop test and the step's settings, wadi2d/solver/stepper.py:106-111.
+__global__ void prestep_kernel(Ctl* ctl) {
+    if (ctl->status != 0 || !(ctl->t < ctl->t_end - 1e-9) || ctl->steps_run >= ctl->max_steps) {
+        ctl->run = 0;
+        return;
+    }
+    ctl->run = 1;
+    const int refresh = ctl->refresh_due || (ctl->nsteps % ctl->dt_every == 0);
+    ctl->refresh_due = 0;
+    const int activate = (int)(ctl->nsteps % ctl->active_every == 0);
+    double dt = ctl->dt;
+    const double rest = ctl->t_end - ctl->t;
+    if (rest < dt) dt = rest;
+    if (ctl->dt_max < dt) dt = ctl->dt_max;
+    ctl->dt_step = dt;
+    ctl->dtf = (float)dt;
+    ctl->want_wave = refresh;
+    ctl->want_wet = activate;
+    ctl->activate = activate && ctl->adaptive;
+    const double t_new = ctl->t + dt;
+    ctl->dt_tally = t_new - ctl->t;
+    ctl->max_time = (float)t_new;
+    ctl->want_max = ctl->max_every > 0 && ((ctl->nsteps + 1) % ctl->max_every == 0);
+    ctl->ticket = 0u;
+}
+
+// A host-driven step (the reference backend's step(dt, want_wave, want_wet)).
+__global__ void setstep_kernel(Ctl* ctl, float dtf, int want_wave, int want_wet, int nact) {
+    ctl->run = 1;
+    ctl->dtf = dtf;
+    ctl->want_wave = want_wave;
+    ctl->want_wet = want_wet;
+    ctl->want_max = 0;
+    ctl->nact = nact;
+    ctl->ticket = 0u;
+    if (want_wave) ctl->wave_max = 0.0f;
+}
+
+// ------------------------------------------------------------------ active-list rebuild (one CTA of 1024)
+
+// Exclusive scan of flags over one 1024-thread CTA; returns this thread's offset and the total in *total.
+__device__ __forceinline__ int block_scan(int flag, int* warp_sums, int* total) {
+    const int tid = threadIdx.x, lane = tid & 31, wid = tid >> 5;
+    int v = flag;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int n = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += n;
+    }
+    if (lane == 31) warp_sums[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        int w = lane < (int)(blockDim.x >> 5) ? warp_sums[lane] : 0;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int n = __shfl_up_sync(0xffffffffu, w, o);
+            if (lane >= o) w += n;
+        }
+        warp_sums[lane] = w;  // inclusive sums of warps
+    }
+    __syncthreads();
+    const int before = (wid > 0 ? warp_sums[wid - 1] : 0) + v - flag;
+    *total = warp_sums[(blockDim.x >> 5) - 1];
+    __syncthreads();
+    return before;
+}
+
+// rebuild_active(check=True), wadi2d/solver/stepper.py:56-92, when ctl->activate: wet or kept tiles and their
+// eight neighbours are active; a tile sleeps after SLEEP_CHECKS checks in a row that did not want it; tiles that
+// join the list are listed in woken for their wet share to be written.
+__global__ void __launch_bounds__(1024) activity_kernel(StepArgs A) {
+    Ctl* ctl = A.ctl;
+    if (!ctl->run || !ctl->activate) return;
+    const int nt = A.ntiles;
+    int* wet_eff = A.scratch;
+    int* flags = A.scratch + nt;
+    for (int t = threadIdx.x; t < nt; t += blockDim.x) wet_eff[t] = t != 0 && (A.wet[t] != 0 || A.keep[t] != 0);
+    __syncthreads();
+    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+        if (t == 0) {
+            flags[0] = 0;
+            continue;
+        }
+        int act = wet_eff[t];
+        for (int n = 0; n < 8; ++n) act |= wet_eff[A.nbr[8 * t + n]];
+        const int cur = A.is_act[t];
+        if (act)
+            A.idle[t] = 0;
+        else
+            A.idle[t] += 1;
+        act |= cur && A.idle[t] < SLEEP_CHECKS;
+        flags[t] = act | ((act && !cur) << 1);
+        A.is_act[t] = act;
+    }
+    __syncthreads();
+    __shared__ int sums[32];
+    int nact = 0, nwoken = 0;
+    for (int base = 0; base < nt; base += blockDim.x) {
+        const int t = base + threadIdx.x;
+        const int f = t < nt ? flags[t] : 0;
+        int tot_a, tot_w;
+        const int oa = block_scan(f & 1, sums, &tot_a);
+        const int ow = block_scan((f >> 1) & 1, sums, &tot_w);
+        if (f & 1) A.active[nact + oa] = t;
+        if (f & 2) A.woken[nwoken + ow] = t;
+        nact += tot_a;
+        nwoken += tot_w;
+    }
+    if (threadIdx.x == 0) {
+        ctl->nact = nact;
+        ctl->nwoken = nwoken;
+    }
+}
+
+// refresh_plan of the listed tiles (wadi2d/solver/gpu/kernels/cells.cu:66-78) from the mean depth h. count < 0:
+// the tiles the device loop's rebuild woke (ctl->nwoken).
+__global__ void __launch_bounds__(256) plan_kernel(StepArgs A, const int32_t* list, int count, const float* h) {
+    Ctl* ctl = A.ctl;
+    if (count < 0) {
+        if (!ctl->run || !ctl->activate) return;
+        count = ctl->nwoken;
+    }
+    for (int a = blockIdx.x; a < count; a += gridDim.x) {
+        const int t = list[a];
+        const int tj = A.tiles[2 * t], ti = A.tiles[2 * t + 1];
+        const int base = (tj * TILE + GY) * A.px + ti * TILE + GX;
+        const float2* pairs_t = A.dtab2 + (size_t)t * (A.rows - 1) * TILE2;
+        for (int c = 0; c < 4; ++c) {
+            const int jj = threadIdx.y * 4 + c, ii = threadIdx.x;
+            const int local = jj * TILE + ii;
+            const int k = base + jj * A.px + ii;
+            A.om[k] = cell_plan(h[k], A.hc[t * TILE2 + local], pairs_t + local, A.rows);
+        }
+    }
+}
+
+// Maxima.update over the active tiles, host-driven (wadi2d/engine/maxima.py:118-130). A's current halves are the
+// state after the step, so u_next here must point at the current u and v.
+__global__ void __launch_bounds__(256) maxima_kernel(StepArgs A, float time, float arrive, float deep, int nact) {
+    for (int a = blockIdx.x; a < nact; a += gridDim.x) {
+        const int t = A.active[a];
+        const int tj = A.tiles[2 * t], ti = A.tiles[2 * t + 1];
+        const int base = (tj * TILE + GY) * A.px + ti * TILE + GX;
+        for (int c = 0; c < 4; ++c) {
+            const int jj = threadIdx.y * 4 + c, ii = threadIdx.x;
+            const int k = base + jj * A.px + ii;
+            envelope(A, t * TILE2 + jj * TILE + ii, k, A.d[k], A.h[k], time, arrive, deep);
+        }
+    }
+}
+
+// Tally.add, host-driven (wadi2d/engine/maxima.py:53-62).
+__global__ void tally_kernel(StepArgs A, double dt) {
+    const int m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= A.ntally) return;
+    const float qv = A.taxis[m] ? A.q[1][A.tface[m]] : A.q[0][A.tface[m]];
+    A.ttotal[m] += dt * (double)(A.tsign[m] * qv);
+}
+
+// ------------------------------------------------------------------ layout converters
+
+// REF_TILE -> NATIVE, own cells of every allocated tile (halo entries of the reference layout are copies).
+__global__ void ref_to_native_kernel(const float* __restrict__ ref, float* __restrict__ nat,
+                                     const int32_t* __restrict__ tiles, int ntiles, int px) {
+    const int t = blockIdx.x + 1;
+    if (t >= ntiles) return;
+    const int tj = tiles[2 * t], ti = tiles[2 * t + 1];
+    for (int idx = threadIdx.x; idx < TILE2; idx += blockDim.x) {
+        const int jj = idx / TILE, ii = idx % TILE;
+        nat[(size_t)(tj * TILE + jj + GY) * px + ti * TILE + ii + GX] = ref[(size_t)t * 1296 + (jj + 2) * 36 + ii + 2];
+    }
+}
+
+// NATIVE -> REF_TILE, every entry of every allocated tile: halos read the neighbour cell they copy (zero beyond
+// the grid or on a missing tile, as the reference's void tile), tile 0 is zero.
+__global__ void native_to_ref_kernel(const float* __restrict__ nat, float* __restrict__ ref,
+                                     const int32_t* __restrict__ tiles, const int32_t* __restrict__ tile_of,
+                                     int ntiles, int ny, int nx, int px) {
+    const int t = blockIdx.x;
+    if (t >= ntiles) return;
+    for (int idx = threadIdx.x; idx < 1296; idx += blockDim.x) {
+        float v = 0.0f;
+        if (t > 0) {
+            const int j = tiles[2 * t] * TILE + idx / 36 - 2;
+            const int i = tiles[2 * t + 1] * TILE + idx % 36 - 2;
+            if (j >= 0 && j < ny && i >= 0 && i < nx && tile_of[(j / TILE) * (nx / TILE) + i / TILE] != 0)
+                v = nat[(size_t)(j + GY) * px + i + GX];
+        }
+        ref[(size_t)t * 1296 + idx] = v;
+    }
+}
+
+// Tables (ntiles,32,32,rows) and (ntiles,32,32,rows,2) -> level-major pairs and quads (ntiles,rows-1,32,32).
+__global__ void pack_tables_kernel(const float* __restrict__ dtab, const float* __restrict__ ftabx,
+                                   const float* __restrict__ ftaby, float2* __restrict__ dtab2,
+                                   float4* __restrict__ fx, float4* __restrict__ fy, int ntiles, int rows) {
+    const size_t n = (size_t)ntiles * (rows - 1) * TILE2;
+    for (size_t o = (size_t)blockIdx.x * blockDim.x + threadIdx.x; o < n; o += (size_t)gridDim.x * blockDim.x) {
+        const size_t local = o % TILE2;
+        const size_t r = (o / TILE2) % (rows - 1);
+        const size_t t = o / ((size_t)TILE2 * (rows - 1));
+        const size_t cell = t * TILE2 + local;
+        dtab2[o] = make_float2(dtab[cell * rows + r], dtab[cell * rows + r + 1]);
+        const float* a = ftabx + cell * rows * 2 + 2 * r;
+        fx[o] = make_float4(a[0], a[1], a[2], a[3]);
+        const float* b = ftaby + cell * rows * 2 + 2 * r;
+        fy[o] = make_float4(b[0], b[1], b[2], b[3]);
+    }
+}
+
+// Boundary marks: clear, then one bit per boundary cell.
+__global__ void bmark_kernel(StepArgs A, int clear_words) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    uint32_t* mark = const_cast<uint32_t*>(A.bmark);
+    if (clear_words > 0) {
+        for (int w = tid; w < clear_words; w += gridDim.x * blockDim.x) mark[w] = 0u;
+        return;
+    }
+    for (int m = tid; m < A.nb; m += gridDim.x * blockDim.x) {
+        const int fid = fid_of_native(A, A.bcell[m]);
+        atomicOr(mark + fid / TILE, 1u << (fid % TILE));
+    }
+}
+
+}  // namespace w2b

@@ -183,6 +183,43 @@ int32_t w2b_tally(void* handle, double dt, void* stream);
 int32_t w2b_advance(void* handle, const W2BStepper* cfg, double t_end, int64_t max_steps, W2BClock* clock,
                     void* stream);
 
+/* Inputs of the table builder (wadi2d/tables/builder.py:131-258; kernels of wadi2d/tables/core.py). Device pointers.
+ * (ny, nx) grids are row-major float64, except mask and walls (uint8, 1 = set). Pixel (r, c) of the grid origin is
+ * z[(r + row_offset) * zw + c + col_offset], indices clipped to the bed as an ArrayBed window is
+ * (wadi2d/tables/builder.py:47-50). k = cell size / pixel <= 32; rows <= 64. */
+typedef struct {
+    const double* z;
+    int64_t zh, zw;
+    int32_t row_offset, col_offset;
+    const double* npix; /* per-pixel Manning n aligned with z (NaN: the cell's own), or NULL */
+    const double* nman; /* (ny, nx) */
+    const double *xcrest, *xlen, *xc, *ycrest, *ylen, *yc; /* CrestFaces, wadi2d/tables/builder.py:62-80 */
+    const uint8_t *xwall, *ywall;                         /* or NULL */
+    const uint8_t* mask;
+    const int32_t* tiles; /* (ntiles, 2) */
+    int32_t ntiles, ny, nx, k, rows, local, margin;
+    double pixel, face_depth_min, face_depth_max, beta, crest_tolerance;
+} W2BTableIn;
+
+/* Outputs: (ntiles, 32, 32[, rows[, 2]]) float32 in the reference's GridTables layout (tile 0 left as the caller
+ * set it: zeros, and ones for efx, efy), and (ny, nx) float64 grids zmin, rel (mean bed over zmin), zfx, zfy (face
+ * inverts) that the caller zeroed. ws: scratch of w2b_table_workspace_doubles(k + 2 margin, ws_threads) doubles,
+ * ws_threads a multiple of 128 (the face kernel's thread count); needed when local != 0. */
+typedef struct {
+    float *hc, *dtab, *efx, *efy, *ftabx, *ftaby, *zcx, *zcy;
+    float *flx, *frx, *glx, *grx, *cwx, *fly, *fry, *gly, *gry, *cwy;
+    double *zmin, *rel, *zfx, *zfy;
+    double* ws;
+    int64_t ws_threads;
+} W2BTableOut;
+
+/* Doubles of table-builder scratch for lines of up to nmax pixels and the given face-kernel thread count. */
+int64_t w2b_table_workspace_doubles(int32_t nmax, int64_t threads);
+
+/* Replaces build_tables (wadi2d/tables/builder.py:131-258): cell tables, face tables (strips, or the local
+ * hydraulic radius when local != 0), centre beds, inverts, closed faces and natural crests, on the GPU. */
+int32_t w2b_build_tables(const W2BTableIn* in, const W2BTableOut* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -29,11 +29,16 @@ def _record(m, extra: dict) -> dict:
     return out
 
 
-def c1_small(api, t_end: float = 600.0, n: int = 64) -> tuple[dict, dict]:
-    """Configuration 1 at n x n: rain on a V-channel plane, free outfall east, CFL 0.9, sleeping tiles on."""
+def c1_small_inputs(api, n: int = 64):
     w = workloads.v_channel_plane(n=n, dx=10.0, k=5, seed=0)
     grid = api.grid(np.ones((w.ny, w.nx), bool), 0.0, 0.0, w.dx)
-    tables = api.tables(grid, w.z, w.dx / w.k, w.manning, True, None, None)
+    return grid, (w.z, w.dx / w.k, w.manning, True, None, None), w
+
+
+def c1_small(api, t_end: float = 600.0, n: int = 64) -> tuple[dict, dict]:
+    """Configuration 1 at n x n: rain on a V-channel plane, free outfall east, CFL 0.9, sleeping tiles on."""
+    grid, targs, w = c1_small_inputs(api, n)
+    tables = api.tables(grid, *targs)
     m = api.model(grid, tables, {"cfl": w.cfl})
     rows, cols = w.outfall
     cells = np.array([m.cell_state_index(int(j), int(i)) for j, i in zip(rows, cols, strict=True)], np.int32)
@@ -60,12 +65,18 @@ def c1_small(api, t_end: float = 600.0, n: int = 64) -> tuple[dict, dict]:
     return _record(m, extra), {"z": w.z, "tables": tables, "grid": grid, "model": m}
 
 
-def dambreak(api, t_end: float = 20.0) -> tuple[dict, dict]:
-    """The reference's rough dam break (tests/solver/test_subgrid.py:95-116) on strips tables, a fixed 0.2 s step."""
+def dambreak_inputs(api):
     nx, ny, k, dx = 60, 40, 6, 10.0
     grid = api.grid(np.ones((ny, nx), bool), 0.0, 0.0, dx)
     z = workloads.rough_dam_break_bed(nx, ny, k, dx, seed=3)
-    tables = api.tables(grid, z, dx / k, 0.03, False, None, None)
+    return grid, (z, dx / k, 0.03, False, None, None), None
+
+
+def dambreak(api, t_end: float = 20.0) -> tuple[dict, dict]:
+    """The reference's rough dam break (tests/solver/test_subgrid.py:95-116) on strips tables, a fixed 0.2 s step."""
+    grid, targs, _ = dambreak_inputs(api)
+    z = targs[0]
+    tables = api.tables(grid, *targs)
     m = api.model(grid, tables, {"dt_every": 1, "dt_max": 0.2})
     h0 = np.zeros(grid.shape)
     h0[:, :30] = 2.0
@@ -137,4 +148,10 @@ def crest(api, t_end: float = 150.0) -> tuple[dict, dict]:
     return _record(m, {}), {"z": z, "tables": tables, "grid": grid, "model": m}
 
 
+def crest_table_inputs(api):
+    grid, z, crest_faces, npix, (nx, ny, k, dx) = crest_inputs(api)
+    return grid, (z, dx / k, 0.04, True, crest_faces, npix), None
+
+
 CASES = {"c1_small": c1_small, "dambreak": dambreak, "crest": crest}
+TABLE_INPUTS = {"c1_small": c1_small_inputs, "dambreak": dambreak_inputs, "crest": crest_table_inputs}

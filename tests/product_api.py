@@ -9,7 +9,7 @@ import numpy as np
 from oracle import oracle as O
 from wadi2d_b200 import tables as T
 from wadi2d_b200.backend import BoundaryCells
-from wadi2d_b200.config import Numerics
+from wadi2d_b200.config import Numerics, Tables
 from wadi2d_b200.grid import TileGrid
 from wadi2d_b200.maxima import Maxima, Tally
 from wadi2d_b200.model import Model
@@ -27,7 +27,7 @@ class B200Api:
 
     def tables(self, grid, z, pixel, manning, local, crest, npix):
         if self.table_source == "gpu":
-            cfg = T.Tables(face_conveyance="local_radius" if local else "strips") if hasattr(T, "Tables") else None
+            cfg = Tables(face_conveyance="local_radius" if local else "strips")
             return T.build_tables(grid, T.ArrayBed(z, pixel), cfg, manning, crest=crest, npix=npix)
         og = O.Grid(grid.x0, grid.y0, grid.dx, grid.mask)
         d = O.build_tables(og, z, pixel, manning, crest=crest, local_radius=local, npix=npix)

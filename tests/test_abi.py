@@ -18,7 +18,7 @@ HEADERS = sorted((Path(__file__).resolve().parents[1] / "include").glob("*.h"))
 def declared() -> list[str]:
     names = []
     for h in HEADERS:
-        names += re.findall(r"^\s*int32_t\s+(w2b_\w+)\s*\(", h.read_text(), flags=re.M)
+        names += re.findall(r"^\s*(?:int32_t|int64_t)\s+(w2b_\w+)\s*\(", h.read_text(), flags=re.M)
     return sorted(set(names))
 
 

@@ -159,17 +159,25 @@ class B200Backend:
             return torch.zeros(int(n), dtype=torch.int32, device=dev)
 
         def up(a, dtype=torch.float32):
+            if isinstance(a, torch.Tensor):
+                return a.reshape(-1).to(device=dev, dtype=dtype).contiguous()
             return torch.as_tensor(np.ascontiguousarray(a).reshape(-1), device=dev).to(dtype).contiguous()
+
+        on_device = getattr(tables, "device_arrays", None) or {}
+
+        def tab(name):
+            """A table array: the builder's device tensor when there is one, else an upload of the host array."""
+            return up(on_device[name] if name in on_device else getattr(tables, name))
 
         t = {}
         for n in ("h", "u", "v", "mx", "my"):
             t[n] = f32(2 * self.ncells).view(2, self.ncells)
         for n in ("d", "qx", "qy", "qx1", "qy1", "res", "src", "om", "zcx", "zcy"):
             t[n] = f32(self.ncells)
-        t["hc"] = up(tables.hc)
+        t["hc"] = tab("hc")
         for ax in "xy":
             for f in ("fl", "fr", "gl", "gr", "ef", "cw"):
-                t[f + ax] = up(getattr(tables, f + ax))
+                t[f + ax] = tab(f + ax)
         t["dtab2"] = f32(nt * (rows - 1) * TILE2 * 2)
         t["ftab4x"] = f32(nt * (rows - 1) * TILE2 * 4)
         t["ftab4y"] = f32(nt * (rows - 1) * TILE2 * 4)
@@ -190,9 +198,9 @@ class B200Backend:
         j = g.tiles[1:, 0, None].astype(np.int64) * TILE + jj[None, :]
         i = g.tiles[1:, 1, None].astype(np.int64) * TILE + ii[None, :]
         self._own = torch.as_tensor(((j + 4) * self.px + i + 32).reshape(-1), device=dev)
-        t["zcx"][self._own] = up(tables.zcx)[TILE2:]
-        t["zcy"][self._own] = up(tables.zcy)[TILE2:]
-        dtab, fx, fy = up(tables.dtab), up(tables.ftabx), up(tables.ftaby)
+        t["zcx"][self._own] = tab("zcx")[TILE2:]
+        t["zcy"][self._own] = tab("zcy")[TILE2:]
+        dtab, fx, fy = tab("dtab"), tab("ftabx"), tab("ftaby")
         stream = self._stream()
         _lib.call("w2b_pack_tables", ctypes.byref(self._desc), dtab.data_ptr(), fx.data_ptr(), fy.data_ptr(),
                   t["dtab2"].data_ptr(), t["ftab4x"].data_ptr(), t["ftab4y"].data_ptr(), stream)  # fmt: skip

@@ -108,7 +108,7 @@ def hbar_at_level(level, zmin: np.ndarray, hc: np.ndarray, dtab: np.ndarray) -> 
     return out
 
 
-def build_tables(grid, bed, cfg=None, manning=0.035, crest=None, lining=None, device=None, npix=None) -> GridTables:
+def build_tables(grid, bed, cfg=None, manning=0.035, crest=None, lining=None, device=None, npix=None):
     """Every static array of the step, built on the GPU from the bed's pixels (wadi2d/tables/builder.py:131-258)."""
     from wadi2d_b200.tablebuild import build_tables_gpu
 

@@ -1,0 +1,331 @@
+#!/usr/bin/env python
+"""Benchmark of the uniform-grid shallow-water step on B200: cell-steps/s on configuration 3.
+
+Workload (one rank): 4096 x 4096 cells at 30 m (16.8 M domain cells, 16,641 tiles of 32 x 32), 4 x 4 pixels a cell,
+the seeded fractal catchment of ``wadi2d_b200.workloads.catchment`` with its tables built on the GPU; a wet start
+(0.05 m of mean depth everywhere) under the storm's peak rain excess, five free outfalls; every tile stepped (the
+reference's "adaptive_active off" headline mode); the envelope every 4 steps and the FP64 outfall tally every step,
+as the reference's monitor takes them. A step is one time step of the whole grid (the device-resident loop,
+graph-captured). Inputs stay resident in HBM (about 15 GB, far beyond the 126 MB L2).
+
+JSON line (rank 0): value = domain cell-steps per second over all ranks (ranks run independent replicas: weak
+scaling, no collective in the data path); roofline of the dominant kernel (the face pass) from CUDA events;
+cpu_baseline = the oracle (a C restatement of the reference's CPU step) on a bounded block of the same workload;
+e2e = the same metric through the C-ABI with host buffers (a source window's rain uploaded from pinned memory, the
+loop run, the clock read back, per 30 s window as the reference's run driver does).
+
+``--impl reference`` times the reference's CPU step (its restatement, the oracle, with every host thread) on the
+same bounded block and prints the same line with "impl": "reference".
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+# Algorithmic bytes per cell-step. The whole step (the fused form): 44 B of state read, 40 B written, 60 B of static
+# scalars, 40 B of table values, 10 B of envelope (5 arrays read and written every 4 steps). The face pass alone:
+# d h u v mx my qx qy read (32 B) + om on refresh steps (4 B / 8), zcx zcy (8 B), 12 face scalars (48 B), two table
+# quads (32 B); u v mx my qx qy written (24 B).
+ALG_STEP = 194.0
+ALG_FACES = 32.0 + 0.5 + 8.0 + 48.0 + 32.0 + 24.0
+FALLBACK_HBM_GBS = 6650.0
+CPU_BLOCK_TILES = 32  # the CPU sample: a 32 x 32-tile block (1,048,576 cells) from the middle of the grid
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=200)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", default="b200", choices=("b200", "reference"))
+    p.add_argument("--n", type=int, default=4096, help="domain side in cells (configuration 3: 4096)")
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--e2e-windows", type=int, default=4)
+    return p.parse_args()
+
+
+def peaks() -> tuple[float, str]:
+    f = ROOT / "MEASURED_PEAKS.json"
+    if f.exists():
+        return float(json.loads(f.read_text())["hbm_gbs"]), "measured"
+    return FALLBACK_HBM_GBS, "fallback"
+
+
+class Clocks:
+    """nvidia-smi sampled every 200 ms during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")  # fmt: skip
+
+    def __init__(self, index: int) -> None:
+        self.index = index
+        self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+        self.proc = None
+
+    def start(self) -> None:
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.index)], stdout=self.file, stderr=subprocess.DEVNULL,
+            )  # fmt: skip
+        except OSError:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        self.proc.wait(timeout=10)
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
+        sm, mx, reasons = [], [], set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                mx.append(float(r[2]))
+            except (ValueError, IndexError):
+                continue
+            for name, v in zip(names, r[5:9], strict=False):
+                if v.strip().lower() == "active":
+                    reasons.add(name)
+        os.unlink(self.file.name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}  # fmt: skip
+
+
+def build_workload(n: int, device):
+    """Configuration 3 on the GPU: catchment, tables, model, outfalls, wet start under peak rain."""
+    from wadi2d_b200 import workloads
+    from wadi2d_b200.backend import BoundaryCells
+    from wadi2d_b200.config import Numerics, Tables
+    from wadi2d_b200.grid import TileGrid
+    from wadi2d_b200.maxima import Maxima, Tally
+    from wadi2d_b200.model import Model
+    from wadi2d_b200.tables import ArrayBed, build_tables
+
+    c = workloads.catchment(n=n, device=device)
+    grid = TileGrid.from_mask(np.ones((n, n), bool), 0.0, 0.0, c.dx)
+    tables = build_tables(grid, ArrayBed(c.z, c.dx / c.k), Tables(), c.manning, device=device)
+    del c.z
+    m = Model(tables, Numerics())
+    m.stepper.adaptive_active = False
+    rows, cols = c.boundary_cells()
+    cells = np.array([m.cell_state_index(int(j), int(i)) for j, i in zip(rows, cols, strict=True)], np.int32)
+    nb = cells.size
+    m.set_boundary(BoundaryCells(cells, cells.copy(), np.ones(nb, np.int32), np.zeros(nb, np.float32),
+                                 np.zeros(nb, np.float32)))  # fmt: skip
+    m.set_depth(np.where(grid.mask, 0.05, 0.0))
+    # rain excess at the hyetograph's peak (2 D / T), less the constant loss, m/s
+    peak_mm_h = 2.0 * c.rain_mm / (c.storm_s / 3600.0)
+    rate = np.maximum(peak_mm_h - c.constant_loss_mm_h, 0.0) / 3.6e6
+    m.set_source(np.where(grid.mask, rate, 0.0))
+    # outflow faces of the outfall cells (east/south faces of the rim cells are their own west/north faces)
+    maxima = Maxima(m, 0.1, 0.05, every=4)
+    tally = Tally(m, cells.astype(np.int64), np.ones(nb), np.zeros(0, np.int64), np.zeros(0))
+    return m, c, grid, tables, maxima, tally, rate
+
+
+def cpu_sample(tables, grid, rate, seconds: float, threads: int, steps: int | None = None, warmup: int = 1):
+    """The oracle on a 32 x 32-tile block cut from the middle of the workload: cell-steps/s on ``threads`` host
+    threads, over about ``seconds`` (or exactly ``steps``) of stepping."""
+    from oracle import oracle as O
+
+    O.threads(threads)
+    B = CPU_BLOCK_TILES
+    nty, ntx = grid.tile_of.shape
+    tj0, ti0 = (nty - B) // 2, (ntx - B) // 2
+    ids = grid.tile_of[tj0 : tj0 + B, ti0 : ti0 + B].reshape(-1)
+    mask = np.ones((B * 32, B * 32), bool)
+    og = O.Grid(0.0, 0.0, grid.dx, mask)
+    order = ids[(og.tiles[1:, 0]) * B + og.tiles[1:, 1]]
+    dev = tables.device_arrays
+    import torch
+
+    sel = torch.as_tensor(np.concatenate(([0], order)), device=dev["hc"].device)
+    sub = {n: dev[n].index_select(0, sel).cpu().numpy() for n in dev if n not in ("zmin", "zbar")}
+    sub["rows"] = tables.rows
+    sub["zmin"] = np.zeros(mask.shape)
+    m = O.Model(og, sub, O.Numerics())
+    m.adaptive_active = False
+    m.set_depth(np.full(mask.shape, 0.05))
+    r = rate[tj0 * 32 : (tj0 + B) * 32, ti0 * 32 : (ti0 + B) * 32]
+    m.set_source(r)
+    cells = mask.size
+    for _ in range(warmup):
+        m.advance(m.t + m.dt * 0.999)
+    n0, t0 = m.nsteps, time.perf_counter()
+    while True:
+        m.advance(m.t + m.dt * 0.999)
+        done = m.nsteps - n0
+        el = time.perf_counter() - t0
+        if (steps is not None and done >= steps) or (steps is None and el >= seconds and done >= 3):
+            break
+    return cells * done / el, done, el, cells
+
+
+def run_reference(args) -> None:
+    """The reference arm: its CPU step (the oracle) on every host thread, on the bounded block."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import torch
+
+    threads = os.cpu_count() or 1
+    dev = torch.device("cuda", 0) if torch.cuda.is_available() else torch.device("cpu")
+    _, _, grid, tables, _, _, rate = build_workload(args.n, dev)
+    value, done, el, cells = cpu_sample(tables, grid, rate, 0.0, threads, steps=args.steps, warmup=args.warmup)
+    sample = f"{CPU_BLOCK_TILES}x{CPU_BLOCK_TILES} tiles ({cells} cells) of the workload, {done} steps"
+    line = {
+        "impl": "reference", "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / max(done, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded fractal catchment, lognormal storm)",
+        "config": {"workload": f"configuration 3, {args.n}x{args.n} cells at 30 m, bounded CPU sample", "sample": sample},
+        "cpu_baseline": {"value": value, "unit": "cell-steps/s", "cores": threads, "kind": "port", "sample": sample},
+        "e2e": {"value": value, "unit": "cell-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
+def main() -> None:
+    args = parse()
+    if args.impl == "reference":
+        run_reference(args)
+        return
+    import torch
+    import torch.distributed as dist
+
+    from wadi2d_b200 import _lib
+
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
+    m, c, grid, tables, maxima, tally, rate = build_workload(args.n, dev)
+    b = m.backend
+    cells = args.n * args.n
+    tile_cells = (grid.ntiles - 1) * 1024
+    stream = torch.cuda.current_stream(dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    # warm-up: the graph capture and the first steps
+    m.run(1e12, maxima=maxima, tally=tally, max_steps=max(args.warmup, 3))
+    barrier()
+    phys = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")
+    clocks = Clocks(int(phys[local]) if len(phys) > local and phys[local].strip().isdigit() else local)
+    clocks.start()
+    time.sleep(0.4)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    n0 = m.stepper.nsteps
+    e0.record(stream)
+    m.run(1e12, maxima=maxima, tally=tally, max_steps=args.steps)
+    e1.record(stream)
+    barrier()
+    clk = clocks.stop()
+    ran = m.stepper.nsteps - n0
+    ms = e0.elapsed_time(e1)
+    if world > 1:
+        t = torch.tensor([ms], device=dev, dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    value = world * cells * ran / (ms / 1e3)
+
+    # the face pass on its own, CUDA events on its stream (the same state, continuing)
+    import ctypes
+
+    times = (ctypes.c_float * 3)()
+    faces_ms, update_ms = [], []
+    for s in range(16):
+        want_wave = s % 8 == 0
+        dt = float(np.float32(m.stepper.dt))
+        _lib.call("w2b_step_timed", b.handle, dt, int(want_wave), 0, stream.cuda_stream, times)
+        faces_ms.append(times[0])
+        update_ms.append(times[1])
+    faces = statistics.mean(faces_ms)
+    hbm, peak_kind = peaks()
+    achieved = ALG_FACES * tile_cells / (faces / 1e3) / 1e9
+    traffic = None
+    tf = ROOT / "profiles" / "faces_kernel_traffic.json"
+    if tf.exists():
+        tr = json.loads(tf.read_text())
+        traffic = tr["bytes_per_cell"] * tile_cells
+    roofline = {"kernel": "faces_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+                "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": traffic,
+                "alg_bytes_per_cell": ALG_FACES, "launch_ms": faces,
+                "update_kernel_ms": statistics.mean(update_ms),
+                "step_alg_bytes_per_cell": ALG_STEP,
+                "step_frac": (cells * ran / (ms / 1e3)) * ALG_STEP / 1e9 / hbm}  # fmt: skip
+
+    # end to end through the C-ABI with host buffers: per 30 s window, the window's rain from pinned memory
+    src_native = b.native("src").cpu().pin_memory()
+    win = 30.0
+    h2d = d2h = 0
+    torch.cuda.synchronize(dev)
+    w0 = time.perf_counter()
+    s0 = m.stepper.nsteps
+    for _ in range(args.e2e_windows):
+        _lib.call("w2b_set_field", b.handle, _lib.FIELD_ID["src"], src_native.data_ptr(), _lib.LAYOUT_NATIVE, 1,
+                  stream.cuda_stream)  # fmt: skip
+        h2d += src_native.numel() * 4
+        m.run(m.stepper.t + win, maxima=maxima, tally=tally)
+        d2h += ctypes.sizeof(_lib.Clock)
+    torch.cuda.synchronize(dev)
+    e2e_s = time.perf_counter() - w0
+    e2e_steps = m.stepper.nsteps - s0
+    e2e = {"value": world * cells * e2e_steps / e2e_s, "unit": "cell-steps/s",
+           "h2d_bytes_per_step": h2d / max(e2e_steps, 1), "d2h_bytes_per_step": d2h / max(e2e_steps, 1),
+           "windows": args.e2e_windows, "steps": e2e_steps}  # fmt: skip
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        threads = os.cpu_count() or 1
+        cv, done, el, ccells = cpu_sample(tables, grid, rate, args.cpu_seconds, threads)
+        cpu = {"value": cv, "unit": "cell-steps/s", "cores": threads, "kind": "port",
+               "sample": f"{CPU_BLOCK_TILES}x{CPU_BLOCK_TILES} tiles ({ccells} cells) of the workload, {done} steps "
+                         f"in {el:.1f} s"}  # fmt: skip
+    if world > 1:
+        dist.barrier()
+    if rank == 0:
+        wet = float((m.field("h") > 0).sum()) / cells
+        line = {
+            "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": ran,
+            "warmup": args.warmup, "ms_per_step": ms / ran, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded fractal catchment, lognormal storm)",
+            "config": {"workload": f"configuration 3: {args.n}x{args.n} cells at 30 m, 4x4 pixels, wet start under peak "
+                                   "rain, every tile stepped, envelope every 4 steps, FP64 tally every step",
+                       "cells": cells, "tiles": grid.ntiles - 1, "wet_fraction": wet, "cfl": m.num.cfl,
+                       "l2": "inputs larger than L2 (about 15 GB resident)", "parallelism": f"replicas x{world}",
+                       "loop": "device-resident, CUDA graphs of 16 steps"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "gpu_launches": 6 * ran,
+        }  # fmt: skip
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

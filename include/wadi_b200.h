@@ -157,6 +157,10 @@ int32_t w2b_set_tally(void* handle, int32_t n, const int32_t* face, const int32_
 /* Replaces step (wadi2d/solver/gpu/backend.py:151-188): faces, positivity, update, boundary, then the swap. */
 int32_t w2b_step(void* handle, float dt, int32_t want_wave, int32_t want_wet, void* stream);
 
+/* w2b_step with CUDA events around its kernels on the stream: ms[0] face pass, ms[1] update pass, ms[2] boundary
+ * pass, in milliseconds (synchronises the stream). For measurement. */
+int32_t w2b_step_timed(void* handle, float dt, int32_t want_wave, int32_t want_wet, void* stream, float* ms);
+
 /* Replaces max_wave / wet_flags (wadi2d/solver/gpu/backend.py:196-200): copy to host, synchronising the stream. */
 int32_t w2b_max_wave(void* handle, float* out, void* stream);
 int32_t w2b_wet_flags(void* handle, int32_t* out, void* stream);

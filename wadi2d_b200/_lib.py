@@ -76,6 +76,7 @@ _SIGNATURES = {
     "w2b_set_boundary": [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp],
     "w2b_set_tally": [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp],
     "w2b_step": [c_vp, c_f32, c_i32, c_i32, c_vp],
+    "w2b_step_timed": [c_vp, c_f32, c_i32, c_i32, c_vp, ctypes.POINTER(c_f32)],
     "w2b_max_wave": [c_vp, ctypes.POINTER(c_f32), c_vp],
     "w2b_wet_flags": [c_vp, c_vp, c_vp],
     "w2b_refresh_plan": [c_vp, c_vp, c_i32, c_vp],
@@ -85,6 +86,7 @@ _SIGNATURES = {
     "w2b_maxima": [c_vp, c_f32, c_f32, c_f32, c_vp],
     "w2b_tally": [c_vp, c_f64, c_vp],
     "w2b_advance": [c_vp, ctypes.POINTER(Stepper), c_f64, c_i64, ctypes.POINTER(Clock), c_vp],
+    "w2b_build_tables": [c_vp, c_vp, c_vp],
 }
 
 _lib = None

@@ -320,6 +320,33 @@ int32_t w2b_step(void* handle, float dt, int32_t want_wave, int32_t want_wet, vo
     return W2B_OK;
 }
 
+int32_t w2b_step_timed(void* handle, float dt, int32_t want_wave, int32_t want_wet, void* stream, float* ms) {
+    if (!handle || !ms) return W2B_EINVAL;
+    Handle* H = static_cast<Handle*>(handle);
+    cudaStream_t s = (cudaStream_t)stream;
+    if (H->nact == 0) return W2B_EINVAL;
+    cudaEvent_t ev[4];
+    for (auto& e : ev) CK(cudaEventCreate(&e));
+    if (want_wave) CK(cudaMemsetAsync(H->B.wave, 0, sizeof(float) * H->g.ntiles, s));
+    setstep_kernel<<<1, 1, 0, s>>>(H->ctl(), dt, want_wave, want_wet, H->nact);
+    const StepArgs A = make_args(*H, H->cur);
+    const dim3 blk(32, 8);
+    const int grid = blocks_for(*H, H->nact);
+    CK(cudaEventRecord(ev[0], s));
+    faces_kernel<<<grid, blk, 0, s>>>(A);
+    CK(cudaEventRecord(ev[1], s));
+    update_kernel<<<grid, blk, 0, s>>>(A);
+    CK(cudaEventRecord(ev[2], s));
+    if (H->nb) boundary_kernel<<<1, 256, 0, s>>>(A, 0);
+    CK(cudaEventRecord(ev[3], s));
+    CKL("w2b_step_timed");
+    H->cur ^= 1;
+    CK(cudaEventSynchronize(ev[3]));
+    for (int e = 0; e < 3; ++e) CK(cudaEventElapsedTime(ms + e, ev[e], ev[e + 1]));
+    for (auto& e : ev) cudaEventDestroy(e);
+    return W2B_OK;
+}
+
 int32_t w2b_max_wave(void* handle, float* out, void* stream) {
     if (!handle || !out) return W2B_EINVAL;
     Handle* H = static_cast<Handle*>(handle);

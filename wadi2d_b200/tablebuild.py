@@ -36,7 +36,6 @@ class TableOut(ctypes.Structure):
     ]
 
 
-_lib.lib()
 _L = _lib.lib()
 _L.w2b_build_tables.argtypes = [ctypes.POINTER(TableIn), ctypes.POINTER(TableOut), ctypes.c_void_p]
 _L.w2b_build_tables.restype = ctypes.c_int32
@@ -87,10 +86,15 @@ def build_tables_gpu(grid: TileGrid, bed, cfg=None, manning=0.035, crest=None, l
         raise ValueError(f"cell size {grid.dx} is not a multiple of the pixel {pixel}")
     ny, nx = grid.shape
     nt, rows = grid.ntiles, int(cfg.rows)
-    z = np.asarray(bed.z, np.float64)
+    if isinstance(bed.z, torch.Tensor):
+        zt = bed.z.to(device=dev, dtype=torch.float64).contiguous()
+        zshape = tuple(zt.shape)
+    else:
+        z = np.asarray(bed.z, np.float64)
+        zshape = z.shape
     if lining is not None and npix is None:
-        npix = np.full(z.shape, np.nan)
-        lining(z, npix, 0, 0)
+        npix = np.full(zshape, np.nan)
+        lining(np.asarray(bed.z.cpu() if isinstance(bed.z, torch.Tensor) else z), npix, 0, 0)
 
     def d64(a):
         return torch.as_tensor(np.ascontiguousarray(a, np.float64), device=dev)
@@ -98,7 +102,8 @@ def build_tables_gpu(grid: TileGrid, bed, cfg=None, manning=0.035, crest=None, l
     def u8(a):
         return torch.as_tensor(np.ascontiguousarray(a, np.uint8), device=dev)
 
-    zt = d64(z)
+    if not isinstance(bed.z, torch.Tensor):
+        zt = d64(z)
     npt = d64(npix) if npix is not None else None
     nman = d64(np.full((ny, nx), float(manning)) if np.isscalar(manning) else manning)
     if crest is None:
@@ -122,7 +127,7 @@ def build_tables_gpu(grid: TileGrid, bed, cfg=None, manning=0.035, crest=None, l
         out[n] = torch.full(shape, 1.0 if n in ("efx", "efy") else 0.0, dtype=torch.float32, device=dev)
     dense = {n: torch.zeros((ny, nx), dtype=torch.float64, device=dev) for n in ("zmin", "rel", "zfx", "zfy")}
     local = cfg.face_conveyance == "local_radius"
-    margin = tile_margin(cfg, pixel, max(z.shape))
+    margin = tile_margin(cfg, pixel, max(zshape))
     nmax = k + 2 * margin
     threads = 148 * 8 * 128
     per_thread = int(_L.w2b_table_workspace_doubles(nmax, 1)) * 8
@@ -134,7 +139,7 @@ def build_tables_gpu(grid: TileGrid, bed, cfg=None, manning=0.035, crest=None, l
         return None if t is None else t.data_ptr()
 
     tin = TableIn(
-        zt.data_ptr(), z.shape[0], z.shape[1], int(getattr(bed, "row_offset", 0)), int(getattr(bed, "col_offset", 0)),
+        zt.data_ptr(), zshape[0], zshape[1], int(getattr(bed, "row_offset", 0)), int(getattr(bed, "col_offset", 0)),
         ptr(npt), nman.data_ptr(), *(crt[n].data_ptr() for n in ("xcrest", "xlen", "xc", "ycrest", "ylen", "yc")),
         ptr(wt[0]), ptr(wt[1]), mask.data_ptr(), tiles.data_ptr(), nt, ny, nx, k, rows, int(local), margin, pixel,
         float(cfg.face_depth_min), float(cfg.face_depth_max), float(cfg.local_radius_beta), float(cfg.crest_tolerance),

@@ -79,3 +79,124 @@ def rough_dam_break_bed(nx: int, ny: int, k: int, dx: float, seed: int = 3) -> n
     pny = 32 * int(np.ceil((ny + 2) / 32))
     pnx = 32 * int(np.ceil((nx + 2) / 32))
     return gaussian_filter(rng.normal(0, 1.0, (pny * k + 2, pnx * k + 2)), 5) * 30 + 200.0
+
+
+@dataclass
+class Catchment:
+    """Configuration 3's inputs on a padded grid. ``z`` is a float64 tensor of pixels (on the generating device)."""
+
+    n: int
+    dx: float
+    k: int
+    z: object
+    manning: float
+    outfalls: list
+    """(rows, columns) of each free outfall's cells, padded coordinates."""
+    rain_mm: np.ndarray
+    """(ny, nx) storm depth per cell, mm: a lognormal field on 1 km pixels (0 off the domain)."""
+    storm_s: float
+    t_end: float
+    initial_loss_mm: float
+    constant_loss_mm_h: float
+
+    def rain_fraction(self, t: float) -> float:
+        """Cumulative share of the storm depth at time t: a triangular hyetograph peaking at half the storm."""
+        T = self.storm_s
+        if t <= 0.0:
+            return 0.0
+        if t >= T:
+            return 1.0
+        x = t / T
+        return 2.0 * x * x if x <= 0.5 else 1.0 - 2.0 * (1.0 - x) ** 2
+
+    def boundary_cells(self) -> tuple[np.ndarray, np.ndarray]:
+        rows = np.concatenate([r for r, _ in self.outfalls])
+        cols = np.concatenate([c for _, c in self.outfalls])
+        return rows, cols
+
+
+def _fractal_torch(shape, hurst, gen_seed, device):
+    import torch
+
+    g = torch.Generator(device="cpu").manual_seed(int(gen_seed))
+    white = torch.randn(shape, generator=g, dtype=torch.float32).to(device)
+    ny, nx = shape
+    ky = torch.fft.fftfreq(ny, device=device)[:, None]
+    kx = torch.fft.rfftfreq(nx, device=device)[None, :]
+    kk = torch.sqrt(kx * kx + ky * ky)
+    kk[0, 0] = 1.0
+    amp = kk ** (-(hurst + 1.0))
+    amp[0, 0] = 0.0
+    f = torch.fft.irfft2(torch.fft.rfft2(white) * amp, s=(ny, nx))
+    f = f - f.mean()
+    return (f / f.std()).to(torch.float64)
+
+
+def catchment(n: int = 4096, dx: float = 30.0, k: int = 4, seed: int = 7, relief: float = 1500.0,
+              device=None) -> Catchment:  # fmt: skip
+    """Configuration 3: an n x n fractal catchment at ``dx`` (k x k pixels a cell) draining south to an alluvial fan,
+    hydrologically conditioned (every cell drains to an outfall), with 5 free outfalls on its rim; a 1 km lognormal
+    storm (mean 60 mm, CV 0.5) over a 12 h triangular hyetograph, 24 h of recession (36 h), initial loss 10 mm and
+    constant loss 2 mm/h."""
+    import torch
+    import torch.nn.functional as F
+
+    dev = torch.device(device if device is not None else ("cuda" if torch.cuda.is_available() else "cpu"))
+    pad = 32 * int(np.ceil((n + 2) / 32))
+    L = n * dx
+    c = (torch.arange(pad, device=dev, dtype=torch.float64) - 1 + 0.5) * dx
+    Y, X = torch.meshgrid(c, c, indexing="ij")  # y grows south
+    xo, yo = 0.5 * L, L
+    r = torch.sqrt((X - xo) ** 2 + (Y - yo) ** 2) / L
+    base = relief * (0.55 * r**1.2 + 0.12 * torch.abs(X - xo) / L + 0.05 * (1.0 - Y / L))
+    smooth = torch.clamp((r - 0.08) / 0.12, 0.0, 1.0)  # the fan near the outlet is smooth
+    fan = 45.0 * torch.clamp(1.0 - r / 0.15, min=0.0)
+    zc = base + fan + smooth * (0.06 * relief) * _fractal_torch((pad, pad), 0.8, seed, dev)
+    domain = torch.zeros((pad, pad), dtype=torch.bool, device=dev)
+    domain[1 : 1 + n, 1 : 1 + n] = True
+    zc = torch.where(domain, zc, torch.full_like(zc, 1e6))
+    # five outfalls on the rim: the main one at the outlet, and the lowest point of four other rim stretches
+    zh = zc.cpu().numpy()
+    half = 10
+    mid = 1 + n // 2
+    outfalls = [(np.full(2 * half + 1, n), np.arange(mid - half, mid + half + 1))]
+    stretches = [
+        ("row", 1, np.arange(1 + n // 8, 1 + 7 * n // 8)),  # north
+        ("col", 1, np.arange(1 + n // 8, 1 + 7 * n // 8)),  # west
+        ("col", n, np.arange(1 + n // 8, 1 + 7 * n // 8)),  # east
+        ("row", n, np.arange(1 + n // 16, 1 + 5 * n // 16)),  # south-west
+    ]
+    for kind, fixed, span in stretches:
+        prof = zh[fixed, span] if kind == "row" else zh[span, fixed]
+        m = int(span[np.argmin(prof)])
+        seg = np.clip(np.arange(m - 5, m + 6), 1, n)
+        outfalls.append((np.full(seg.size, fixed), seg) if kind == "row" else (seg, np.full(seg.size, fixed)))
+    sink = torch.zeros_like(domain)
+    for rr, cc in outfalls:
+        sink[torch.as_tensor(rr, device=dev), torch.as_tensor(cc, device=dev)] = True
+    # Planchon-Darboux: the least surface over the ground that drains to a sink, 1 mm a cell of grade
+    inf = torch.full_like(zc, float("inf"))
+    W = torch.where(sink, zc, inf)
+    eps = 1e-3
+    for it in range(20 * pad):
+        nb = -F.max_pool2d(-W[None, None], 3, stride=1, padding=1)[0, 0]
+        Wn = torch.where(domain & ~sink, torch.maximum(zc, torch.minimum(W, nb + eps)), W)
+        if it % 64 == 63:
+            if torch.equal(Wn, W):
+                break
+        W = Wn
+    # the conditioned surface, its padding repeating the rim; then pixels: bilinear, plus sub-cell relief
+    zc = F.pad(W[1 : 1 + n, 1 : 1 + n][None, None], (1, pad - n - 1, 1, pad - n - 1), mode="replicate")[0, 0]
+    npx = pad * k
+    zp = F.interpolate(zc[None, None], size=(npx, npx), mode="bilinear", align_corners=False)[0, 0]
+    zp = zp + 1.5 * _fractal_torch((npx, npx), 0.8, seed + 1, dev)
+    # the storm: lognormal depths on 1 km pixels
+    rng = np.random.default_rng(3)
+    sig = np.sqrt(np.log(1.0 + 0.5**2))
+    mu = np.log(60.0) - 0.5 * sig * sig
+    nk = int(np.ceil(L / 1000.0))
+    field = rng.lognormal(mu, sig, (nk, nk))
+    cc = np.clip(((np.arange(pad) - 1 + 0.5) * dx // 1000.0).astype(int), 0, nk - 1)
+    rain = field[np.ix_(cc, cc)]
+    rain[~domain.cpu().numpy()] = 0.0
+    return Catchment(n, dx, k, zp, 0.035, outfalls, rain, 12 * 3600.0, 36 * 3600.0, 10.0, 2.0)

@@ -268,10 +268,11 @@ def main() -> None:
     hbm, peak_kind = peaks()
     achieved = ALG_FACES * tile_cells / (faces / 1e3) / 1e9
     traffic = None
-    tf = ROOT / "profiles" / "faces_kernel_traffic.json"
+    tf = ROOT / "profiles" / "faces_kernel_config3_1024.md"
     if tf.exists():
-        tr = json.loads(tf.read_text())
-        traffic = tr["bytes_per_cell"] * tile_cells
+        for ln in tf.read_text().splitlines():
+            if ln.startswith("traffic_bytes_per_cell:"):
+                traffic = float(ln.split(":")[1]) * tile_cells  # the capture's bytes a cell, scaled to this launch
     roofline = {"kernel": "faces_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": traffic,
                 "alg_bytes_per_cell": ALG_FACES, "launch_ms": faces,

@@ -7,10 +7,14 @@
 #include <cstring>
 #include <new>
 
+#include <cuda.h>
+
 #include "w2b_common.cuh"
 
 namespace w2b {
-__global__ void faces_kernel(StepArgs A);
+cudaError_t faces_setup();
+int faces_occupancy();
+void launch_faces(const TMaps& M, const StepArgs& A, int p, int grid, cudaStream_t s);
 __global__ void update_kernel(StepArgs A);
 __global__ void boundary_kernel(StepArgs A, int control);
 __global__ void prestep_kernel(Ctl* ctl);
@@ -47,7 +51,9 @@ struct Handle {
     const float* tsign = nullptr;
     double* ttotal = nullptr;
     int sms = 148;
-    int step_blocks = 148;  // resident CTAs of the step kernels
+    int step_blocks = 148;   // resident CTAs of the update pass
+    int faces_blocks = 296;  // resident CTAs of the face pass
+    TMaps tmaps;
     unsigned version = 0;   // bumped whenever a graph would capture stale arguments
     Loop loop;
     cudaStream_t cap = nullptr;  // private stream the loop graphs are captured on (a legacy stream cannot be)
@@ -138,6 +144,60 @@ static int cuda_status(cudaError_t e, const char* where) {
 #define CKL(where) CK(cudaGetLastError())
 
 static int blocks_for(const Handle& H, int n) { return n < H.step_blocks ? (n > 0 ? n : 1) : H.step_blocks; }
+static int faces_grid(const Handle& H, int n) { return n < H.faces_blocks ? (n > 0 ? n : 1) : H.faces_blocks; }
+
+// cuTensorMapEncodeTiled, fetched from the driver at run time (so the library does not link libcuda).
+typedef CUresult (*EncodeTiled)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+static int encode_2d(EncodeTiled enc, CUtensorMap* map, const float* base, const W2BGridDesc& g, const W2BLayout& L,
+                     uint32_t bw, uint32_t bh) {
+    if (!base || ((uintptr_t)base & 15)) return W2B_EINVAL;
+    const cuuint64_t dims[2] = {(cuuint64_t)L.px, (cuuint64_t)(g.ny + 2 * L.gy)};
+    const cuuint64_t strides[1] = {(cuuint64_t)L.px * 4};
+    const cuuint32_t box[2] = {bw, bh};
+    const cuuint32_t es[2] = {1, 1};
+    const CUresult r = enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT32, 2, (void*)base, dims, strides, box, es,
+                           CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                           CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    if (r != CUDA_SUCCESS) {
+        fprintf(stderr, "libwadi_b200: cuTensorMapEncodeTiled failed (%d)\n", (int)r);
+        return W2B_ECUDA;
+    }
+    return W2B_OK;
+}
+
+static int build_tmaps(Handle& H) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &q) != cudaSuccess || !fn ||
+        q != cudaDriverEntryPointSuccess)
+        return W2B_ECUDA;
+    EncodeTiled enc = reinterpret_cast<EncodeTiled>(fn);
+    const W2BBuffers& B = H.B;
+    int st = W2B_OK;
+    auto box = [&](CUtensorMap* m, const float* p) {
+        if (st == W2B_OK) st = encode_2d(enc, m, p, H.g, H.L, 40, 36);
+    };
+    auto own = [&](CUtensorMap* m, const float* p) {
+        if (st == W2B_OK) st = encode_2d(enc, m, p, H.g, H.L, 32, 32);
+    };
+    box(&H.tmaps.d, B.d);
+    box(&H.tmaps.qx, B.qx);
+    box(&H.tmaps.qy, B.qy);
+    box(&H.tmaps.om, B.om);
+    box(&H.tmaps.zcx, B.zcx);
+    box(&H.tmaps.zcy, B.zcy);
+    for (int p = 0; p < 2; ++p) {
+        box(&H.tmaps.h[p], B.h[p]);
+        box(&H.tmaps.u[p], B.u[p]);
+        box(&H.tmaps.v[p], B.v[p]);
+        own(&H.tmaps.mx[p], B.mx[p]);
+        own(&H.tmaps.my[p], B.my[p]);
+    }
+    return st;
+}
 
 static void drop_graphs(Handle& H) {
     for (auto& e : H.loop.exec)
@@ -154,7 +214,7 @@ static int launch_loop_step(Handle& H, int p, cudaStream_t s) {
     const dim3 blk(32, 8);
     const int grid = blocks_for(H, H.g.ntiles - 1);
     prestep_kernel<<<1, 1, 0, s>>>(A.ctl);
-    faces_kernel<<<grid, blk, 0, s>>>(A);
+    launch_faces(H.tmaps, A, p, faces_grid(H, H.g.ntiles - 1), s);
     update_kernel<<<grid, blk, 0, s>>>(A);
     boundary_kernel<<<1, 256, 0, s>>>(A, 1);
     activity_kernel<<<1, 1024, 0, s>>>(A);
@@ -214,11 +274,18 @@ int32_t w2b_create(const W2BGridDesc* grid, const W2BParams* params, const W2BBu
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&H->sms, cudaDevAttrMultiProcessorCount, dev);
     int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, faces_kernel, 256, 0);
-    int occ2 = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ2, update_kernel, 256, 0);
-    occ = occ2 < occ ? occ2 : occ;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, update_kernel, 256, 0);
     H->step_blocks = H->sms * (occ > 0 ? occ : 1);
+    if (faces_setup() != cudaSuccess) {
+        delete H;
+        return cuda_status(cudaGetLastError(), "w2b_create faces_setup");
+    }
+    const int focc = faces_occupancy();
+    H->faces_blocks = H->sms * (focc > 0 ? focc : 1);
+    if (build_tmaps(*H) != W2B_OK) {
+        delete H;
+        return W2B_ECUDA;
+    }
     H->nact = grid->ntiles - 1;
     if (cudaStreamCreateWithFlags(&H->cap, cudaStreamNonBlocking) != cudaSuccess) {
         delete H;
@@ -312,7 +379,7 @@ int32_t w2b_step(void* handle, float dt, int32_t want_wave, int32_t want_wet, vo
     const StepArgs A = make_args(*H, H->cur);
     const dim3 blk(32, 8);
     const int grid = blocks_for(*H, H->nact);
-    faces_kernel<<<grid, blk, 0, s>>>(A);
+    launch_faces(H->tmaps, A, H->cur, faces_grid(*H, H->nact), s);
     update_kernel<<<grid, blk, 0, s>>>(A);
     if (H->nb) boundary_kernel<<<1, 256, 0, s>>>(A, 0);
     CKL("w2b_step");
@@ -333,7 +400,7 @@ int32_t w2b_step_timed(void* handle, float dt, int32_t want_wave, int32_t want_w
     const dim3 blk(32, 8);
     const int grid = blocks_for(*H, H->nact);
     CK(cudaEventRecord(ev[0], s));
-    faces_kernel<<<grid, blk, 0, s>>>(A);
+    launch_faces(H->tmaps, A, H->cur, faces_grid(*H, H->nact), s);
     CK(cudaEventRecord(ev[1], s));
     update_kernel<<<grid, blk, 0, s>>>(A);
     CK(cudaEventRecord(ev[2], s));
@@ -350,9 +417,11 @@ int32_t w2b_step_timed(void* handle, float dt, int32_t want_wave, int32_t want_w
 int32_t w2b_max_wave(void* handle, float* out, void* stream) {
     if (!handle || !out) return W2B_EINVAL;
     Handle* H = static_cast<Handle*>(handle);
+    int32_t status = 0;
     CK(cudaMemcpyAsync(out, &H->ctl()->wave_max, sizeof(float), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    CK(cudaMemcpyAsync(&status, &H->ctl()->status, sizeof(int32_t), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
     CK(cudaStreamSynchronize((cudaStream_t)stream));
-    return W2B_OK;
+    return status == W2B_ETIMEOUT ? W2B_ETIMEOUT : W2B_OK;
 }
 
 int32_t w2b_wet_flags(void* handle, int32_t* out, void* stream) {

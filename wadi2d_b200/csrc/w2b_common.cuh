@@ -5,6 +5,7 @@
 #pragma once
 
 #include <cstdint>
+#include <cuda.h>
 #include <cuda_runtime.h>
 
 #include "wadi_b200.h"
@@ -101,6 +102,13 @@ struct StepArgs {
     const float* __restrict__ tsign;
     double* __restrict__ ttotal;
     Ctl* ctl;
+};
+
+// Tensor maps of the NATIVE state arrays for the face pass's TMA boxes: 40 x 36 floats (the tile, two cells of halo
+// north and south, four west and east so that the box's first column stays 16-byte aligned), and 32 x 32 for the
+// momenta, which the face pass reads at own faces only. Ping-pong pairs have one map a half.
+struct TMaps {
+    CUtensorMap d, h[2], u[2], v[2], qx, qy, om, zcx, zcy, mx[2], my[2];
 };
 
 // ------------------------------------------------------------------ float32 helpers

@@ -12,119 +12,175 @@
 #include <cstdio>
 
 #include "w2b_common.cuh"
+#include "w2b_tma.cuh"
 
 namespace w2b {
 
 // ------------------------------------------------------------------ face pass
 
-// One face: AX 0 is the west (x) face of cell k, AX 1 its north (y) face. Returns the wave speed.
-template <int AX>
-__device__ __forceinline__ float face_step(const StepArgs& A, int k, int fid, int t, int local, float dt,
-                                           int want_wave) {
-    const W2BParams& P = A.P;
-    const int s = AX == 0 ? 1 : A.px;  // along the normal
-    const int p = AX == 0 ? A.px : 1;  // across it
-    const float* __restrict__ u = A.u[AX];
-    const float* __restrict__ m = A.m[AX];
-    const float* __restrict__ q = A.q[AX];
-    const float* __restrict__ qp = A.q[1 - AX];
-    const float* __restrict__ vp = A.u[1 - AX];
-    const float* __restrict__ d = A.d;
-    const float* __restrict__ h = A.h;
-    const float ZERO = 0.0f, HALF = 0.5f, ONE = 1.0f;
-    const float dx = P.dx;
-    const float span = dx;
+// Shared-memory image of one tile for the face pass. Boxes of 40 x 36 floats hold the tile with 2 cells of halo north
+// and south and 4 west and east (the TMA box starts on a 16-byte boundary); own cell (j, i) sits at box (j + 2, i + 4).
+constexpr int BOXW = 40, BOXH = 36, BOX = BOXW * BOXH;
+constexpr int F_D = 0, F_H = 1, F_U = 2, F_V = 3, F_QX = 4, F_QY = 5, F_OM = 6, F_ZCX = 7, F_ZCY = 8, NBOX = 9;
+constexpr int SM_M = NBOX * BOX;          // mx, my: 32 x 32 each
+constexpr int SM_ST = SM_M + 2 * TILE2;   // the 12 static face scalars of the tile, 32 x 32 each
+constexpr int SM_FLOATS = SM_ST + 12 * TILE2;
+constexpr int FACES_SMEM = SM_FLOATS * 4;  // 109,184 bytes: two CTAs a SM
+constexpr int FACES_THREADS = 512;
 
-    const float fl = __ldg(A.fl[AX] + fid);
-    const float fr = __ldg(A.fr[AX] + fid);
-    const float e_l = __ldg(d + k - s) - fl;
-    const float e_r = __ldg(d + k) - fr;
-    const float uf = __ldg(u + k);
-    const float e_lp = fmax32(e_l, ZERO);
-    const float e_rp = fmax32(e_r, ZERO);
-    const bool from_left = uf > ZERO || (uf == ZERO && e_l >= e_r);
-    const float eup = from_left ? e_lp : e_rp;
-    if (eup <= P.e_wet) {
-        A.u_next[AX][k] = ZERO;
-        A.m_next[AX][k] = ZERO;
-        A.q1[AX][k] = ZERO;
-        return ZERO;
-    }
-    const float cwf = __ldg(A.cw[AX] + fid);
-    const float top = __ldg(A.ef[AX] + fid);
-    float eface = eup;
-    if (P.carry && cwf == ZERO) {
-        const float dz = from_left ? __ldg(A.zc[AX] + k - s) - fl : __ldg(A.zc[AX] + k) - fr;
+// What the first part of a face computes: the upwind choice, the face depth, the table row, and the row's quad,
+// whose load is issued there and consumed after the table-free momentum terms.
+struct FaceA {
+    float e_l, e_r, e_lp, e_rp, uf, eup, eface, top, cwf, fl, fr;
+    int r;
+    bool from_left, live, above;
+    float4 q;
+};
+
+// Part A of the face of axis AX at box index b (wadi2d/solver/gpu/kernels/faces.cu:19-44).
+template <int AX>
+__device__ __forceinline__ void face_a(const float* sm, int b, int local, const StepArgs& A, int t, FaceA& F) {
+    constexpr int S = AX == 0 ? 1 : BOXW;
+    const W2BParams& P = A.P;
+    const float* D = sm + F_D * BOX;
+    const float* U = sm + (AX == 0 ? F_U : F_V) * BOX;
+    const float* st = sm + SM_ST + AX * 6 * TILE2;
+    F.fl = st[0 * TILE2 + local];
+    F.fr = st[1 * TILE2 + local];
+    F.e_l = D[b - S] - F.fl;
+    F.e_r = D[b] - F.fr;
+    F.uf = U[b];
+    F.e_lp = fmax32(F.e_l, 0.0f);
+    F.e_rp = fmax32(F.e_r, 0.0f);
+    F.from_left = F.uf > 0.0f || (F.uf == 0.0f && F.e_l >= F.e_r);
+    F.eup = F.from_left ? F.e_lp : F.e_rp;
+    F.live = !(F.eup <= P.e_wet);
+    if (!F.live) return;
+    F.cwf = st[5 * TILE2 + local];
+    F.top = st[4 * TILE2 + local];
+    F.eface = F.eup;
+    if (P.carry && F.cwf == 0.0f) {
+        const float* ZC = sm + (AX == 0 ? F_ZCX : F_ZCY) * BOX;
+        const float dz = F.from_left ? ZC[b - S] - F.fl : ZC[b] - F.fr;
         if (dz > 1e-6f) {
-            float phi = (eup - 2.0f * dz) / (2.0f * dz);
-            phi = phi < ZERO ? ZERO : (phi > ONE ? ONE : phi);
-            eface = eup - phi * dz;
+            float phi = (F.eup - 2.0f * dz) / (2.0f * dz);
+            phi = phi < 0.0f ? 0.0f : (phi > 1.0f ? 1.0f : phi);
+            F.eface = F.eup - phi * dz;
         }
     }
-    const float4* __restrict__ quads = A.ftab4[AX] + (size_t)t * (A.rows - 1) * TILE2 + local;
-    float area, tt, w;
-    face_lookup(eface, top, quads, A.rows, area, tt, w);
-    const float h_l = __ldg(h + k - s);
-    const float h_r = __ldg(h + k);
+    const int last = A.rows - 1;
+    F.above = F.eface >= F.top;
+    F.r = F.above ? last - 1 : row_of(sqrtf(F.eface / F.top) * (float)last, last);
+    const float4* quads = A.ftab4[AX] + (size_t)t * (A.rows - 1) * TILE2 + local;
+    F.q = __ldg(quads + (size_t)F.r * TILE2);
+}
+
+// Parts B and C: the momentum terms (faces.cu:50-100, table-free), then the lookup, section, friction, crest cap,
+// outputs and wave speed (faces.cu:43-44, :52-63, :102-145). Returns the wave speed.
+template <int AX>
+__device__ __forceinline__ float face_bc(const float* sm, int b, int local, int k, const StepArgs& A, int t,
+                                         const FaceA& F, float dt, int want_wave) {
+    constexpr int S = AX == 0 ? 1 : BOXW;
+    constexpr int PP = AX == 0 ? BOXW : 1;
+    const W2BParams& P = A.P;
+    if (!F.live) {
+        A.u_next[AX][k] = 0.0f;
+        A.m_next[AX][k] = 0.0f;
+        A.q1[AX][k] = 0.0f;
+        return 0.0f;
+    }
+    const float ZERO = 0.0f, HALF = 0.5f, ONE = 1.0f;
+    const float dx = P.dx, span = dx;
+    const float* H = sm + F_H * BOX;
+    const float* U = sm + (AX == 0 ? F_U : F_V) * BOX;
+    const float* VP = sm + (AX == 0 ? F_V : F_U) * BOX;
+    const float* Q = sm + (AX == 0 ? F_QX : F_QY) * BOX;
+    const float* QP = sm + (AX == 0 ? F_QY : F_QX) * BOX;
+    const float* st = sm + SM_ST + AX * 6 * TILE2;
+    const bool from_left = F.from_left;
+    const float uf = F.uf;
+    const float h_l = H[b - S], h_r = H[b];
     const float hup = from_left ? h_l : h_r;
 
-    // [1] section
-    float rho = ONE;
-    float d_eta = e_rp - e_lp;
+    // [1] section: the disconnected drive (the volume-limited section needs the table, below)
+    float d_eta = F.e_rp - F.e_lp;
     if (P.sheet) {
-        const float avol = hup * dx;
-        const float edown = from_left ? e_rp : e_lp;
-        if (avol < area) {
-            const float sub = fmin32(e_lp, e_rp) / fmax32(e_lp, e_rp);
-            const float sub2 = sub * sub;
-            const float alpha = sub2 * sub2;
-            rho = alpha + (ONE - alpha) * avol / area;
-        }
+        const float edown = from_left ? F.e_rp : F.e_lp;
         if (edown <= ZERO) {
-            // [2] disconnected
-            const float g_u = from_left ? __ldg(A.gl[AX] + fid) : __ldg(A.gr[AX] + fid);
-            const float g_d = from_left ? __ldg(A.gr[AX] + fid) : __ldg(A.gl[AX] + fid);
+            const float g_u = from_left ? st[2 * TILE2 + local] : st[3 * TILE2 + local];
+            const float g_d = from_left ? st[3 * TILE2 + local] : st[2 * TILE2 + local];
             const float h_d = from_left ? h_r : h_l;
             const float drop = (hup - g_u) - fmax32(h_d - g_d, HALF * (g_u - g_d));
-            const float level_drop = fabsf(e_l - e_r);
-            const float drive = fmax32(eup, fmin32(drop, level_drop));
+            const float level_drop = fabsf(F.e_l - F.e_r);
+            const float drive = fmax32(F.eup, fmin32(drop, level_drop));
             d_eta = from_left ? -drive : drive;
         }
     }
-
     // [3] momentum fluxes
     const int mirror = P.mirror, second = P.second;
-    const float um = gated(__ldg(u + k - s), uf, mirror);
-    const float up = gated(__ldg(u + k + s), uf, mirror);
-    const float umm = gated(__ldg(u + k - 2 * s), um, mirror);
-    const float upp = gated(__ldg(u + k + 2 * s), up, mirror);
-    const float qk = __ldg(q + k);
-    const float qc_l = HALF * (__ldg(q + k - s) + qk);
-    const float qc_r = HALF * (qk + __ldg(q + k + s));
+    const float um = gated(U[b - S], uf, mirror);
+    const float up = gated(U[b + S], uf, mirror);
+    const float umm = gated(U[b - 2 * S], um, mirror);
+    const float upp = gated(U[b + 2 * S], up, mirror);
+    const float qk = Q[b];
+    const float qc_l = HALF * (Q[b - S] + qk);
+    const float qc_r = HALF * (qk + Q[b + S]);
     const float s_l = qc_l > ZERO ? ustar(um, umm, uf, second) : ustar(uf, up, um, second);
     const float s_r = qc_r > ZERO ? ustar(uf, um, up, second) : ustar(up, upp, uf, second);
     float flux = qc_r * s_r - qc_l * s_l;
-    const float qy_s = HALF * (__ldg(qp + k - s) + __ldg(qp + k));
-    const float qy_n = HALF * (__ldg(qp + k - s + p) + __ldg(qp + k + p));
-    const float u_s = gated(__ldg(u + k - p), uf, mirror);
-    const float u_n = gated(__ldg(u + k + p), uf, mirror);
-    const float uss = gated(__ldg(u + k - 2 * p), u_s, mirror);
-    const float unn = gated(__ldg(u + k + 2 * p), u_n, mirror);
+    const float qy_s = HALF * (QP[b - S] + QP[b]);
+    const float qy_n = HALF * (QP[b - S + PP] + QP[b + PP]);
+    const float u_s = gated(U[b - PP], uf, mirror);
+    const float u_n = gated(U[b + PP], uf, mirror);
+    const float uss = gated(U[b - 2 * PP], u_s, mirror);
+    const float unn = gated(U[b + 2 * PP], u_n, mirror);
     const float us_s = qy_s > ZERO ? ustar(u_s, uss, uf, second) : ustar(uf, u_n, u_s, second);
     const float us_n = qy_n > ZERO ? ustar(uf, u_s, u_n, second) : ustar(u_n, unn, uf, second);
     flux += qy_n * us_n - qy_s * us_s;
-
     // [4] momentum and pressure
     const float abar = HALF * (h_l + h_r) * dx;
     const float press = dt * P.g * d_eta / span;
     float us;
     if (abar > 1e-6f * dx)
-        us = (__ldg(m + k) - dt * flux / span) / abar - press;
+        us = (sm[SM_M + AX * TILE2 + local] - dt * flux / span) / abar - press;
     else
         us = uf - press;
+    const float vb = 0.25f * (VP[b - S] + VP[b] + VP[b - S + PP] + VP[b + PP]);
 
+    // the table lookup from the quad loaded in part A (common.cuh face_lookup)
+    const float top = F.top, e = F.eface;
+    const float m = (float)(A.rows - 1);
+    const float4 q = F.q;
+    float area, tt, w;
+    if (F.above) {
+        const float a1 = q.z, a0 = q.x;
+        const float c = (m - 1.0f) / m;
+        w = (a1 - a0) / (top * (1.0f - c * c));
+        area = a1 + w * (e - top);
+        tt = q.w * (area / fmax32(a1, 1e-12f));
+    } else {
+        const int r = F.r;
+        const float c0 = (float)r / m;
+        const float c1 = (float)(r + 1) / m;
+        const float e0 = c0 * c0 * top;
+        const float de = (c1 * c1 - c0 * c0) * top;
+        const float f = (e - e0) / de;
+        area = q.x + f * (q.z - q.x);
+        tt = q.y + f * (q.w - q.y);
+        w = (q.z - q.x) / de;
+    }
+    // [1] the volume-limited section
+    float rho = ONE;
+    if (P.sheet) {
+        const float avol = hup * dx;
+        if (avol < area) {
+            const float sub = fmin32(F.e_lp, F.e_rp) / fmax32(F.e_lp, F.e_rp);
+            const float sub2 = sub * sub;
+            const float alpha = sub2 * sub2;
+            rho = alpha + (ONE - alpha) * avol / area;
+        }
+    }
     // [5] friction
-    const float vb = 0.25f * (__ldg(vp + k - s) + __ldg(vp + k) + __ldg(vp + k - s + p) + __ldg(vp + k + p));
     const float t3 = tt * tt * tt * cbrt32(tt);
     float fric = area * area / fmax32(t3, 1e-30f);
     if (rho < ONE) fric = fric / fmax32(rho * cbrt32(rho), 1e-12f);
@@ -132,17 +188,17 @@ __device__ __forceinline__ float face_step(const StepArgs& A, int k, int fid, in
     const float sp = sqrtf(us * us + vb * vb);
     float un = 2.0f * us / (ONE + sqrtf(ONE + 4.0f * a * sp));
     if (fabsf(un) > P.u_max) un = un > ZERO ? P.u_max : -P.u_max;
-
     // [6] crest face
     float qn = area * rho * un;
-    float c = cwf;
+    float c = F.cwf;
     if (c != ZERO) {
         float area_c = area, w_c = w;
         if (c < ZERO) {
             c = -c;
             const float ua = from_left ? um : up;
             float tc;
-            face_lookup(eup + HALF * ua * ua / P.g, top, quads, A.rows, area_c, tc, w_c);
+            const float4* quads = A.ftab4[AX] + (size_t)t * (A.rows - 1) * TILE2 + local;
+            face_lookup(F.eup + HALF * ua * ua / P.g, top, quads, A.rows, area_c, tc, w_c);
         }
         const float qc = c * area_c * sqrtf(area_c / fmax32(w_c, 1e-9f));
         if (fabsf(qn) > qc) {
@@ -155,13 +211,14 @@ __device__ __forceinline__ float face_step(const StepArgs& A, int k, int fid, in
     A.q1[AX][k] = qn;
     if (!want_wave) return ZERO;
     if (not_finite(un)) return 1e30f;
-    const float d_left = __ldg(d + k - s);
-    const float d_right = __ldg(d + k);
+    const float* D = sm + F_D * BOX;
+    const float* OM = sm + F_OM * BOX;
+    const float d_left = D[b - S], d_right = D[b];
     const float dup = from_left ? d_left : d_right;
     if (dup <= P.h_cfl) return ZERO;
-    float plan = from_left ? __ldg(A.om + k - s) : __ldg(A.om + k);
+    float plan = from_left ? OM[b - S] : OM[b];
     const float dother = from_left ? d_right : d_left;
-    if (dother > P.h_cfl) plan = fmin32(plan, from_left ? __ldg(A.om + k) : __ldg(A.om + k - s));
+    if (dother > P.h_cfl) plan = fmin32(plan, from_left ? OM[b] : OM[b - S]);
     const float wave = sqrtf(fmax32(P.g * area * rho / (fmax32(plan, P.a_min) * dx), ZERO));
     return fabsf(un) + fmin32(P.lead * fabsf(un - uf), 2.0f * wave) + wave;
 }
@@ -171,53 +228,100 @@ __device__ __forceinline__ float warp_max(float v) {
     return v;
 }
 
-// Block-wide max of v (256 threads); the result is valid in thread 0.
+// Block-wide max of v; the result is valid in thread 0. red holds one entry a warp.
 __device__ __forceinline__ float block_max(float v, float* red) {
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int nw = (int)(blockDim.x * blockDim.y) / 32;
     v = warp_max(v);
     if ((tid & 31) == 0) red[tid >> 5] = v;
     __syncthreads();
     float r = 0.0f;
     if (tid < 32) {
-        r = tid < (int)(blockDim.x * blockDim.y) / 32 ? red[tid] : 0.0f;
+        r = tid < nw ? red[tid] : 0.0f;
         r = warp_max(r);
     }
     __syncthreads();
     return r;
 }
 
-__global__ void __launch_bounds__(256) faces_kernel(StepArgs A) {
+// The face pass: both own faces of every cell of the active tiles (wadi2d/solver/gpu/kernels/faces.cu:148-175).
+// Each CTA (16 warps, a warp a tile row, two rows a warp) stages a tile with TMA: nine 40 x 36 state boxes, the two
+// momenta, and the tile's twelve static face scalars as bulk copies; the per-tile wave maxima are reduced at the end
+// by the last CTA to finish. p is the parity of the ping-pong halves.
+__global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_constant__ TMaps M, StepArgs A, int p) {
+    extern __shared__ __align__(128) float sm[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ float red[32];
+    __shared__ bool last;
     Ctl* ctl = A.ctl;
     if (!ctl->run) return;
     const int nact = ctl->nact;
     const float dt = ctl->dtf;
     const int want_wave = ctl->want_wave;
-    __shared__ float red[8];
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    const uint32_t bytes = (uint32_t)((NBOX - (want_wave ? 0 : 1)) * BOX + 14 * TILE2) * 4u;
+    const float* statics[12] = {A.fl[0], A.fr[0], A.gl[0], A.gr[0], A.ef[0], A.cw[0],
+                                A.fl[1], A.fr[1], A.gl[1], A.gr[1], A.ef[1], A.cw[1]};
+    uint32_t phase = 0;
+    const int lane = tid & 31, warp = tid >> 5;
     for (int a = blockIdx.x; a < nact; a += gridDim.x) {
         const int t = A.active[a];
         const int tj = A.tiles[2 * t], ti = A.tiles[2 * t + 1];
+        if (tid == 0) {
+            fence_proxy_async();
+            mbar_expect_tx(&bar, bytes);
+            const int x0 = ti * TILE + GX - 4, y0 = tj * TILE + GY - 2;
+            tma_load_2d(sm + F_D * BOX, &M.d, x0, y0, &bar);
+            tma_load_2d(sm + F_H * BOX, &M.h[p], x0, y0, &bar);
+            tma_load_2d(sm + F_U * BOX, &M.u[p], x0, y0, &bar);
+            tma_load_2d(sm + F_V * BOX, &M.v[p], x0, y0, &bar);
+            tma_load_2d(sm + F_QX * BOX, &M.qx, x0, y0, &bar);
+            tma_load_2d(sm + F_QY * BOX, &M.qy, x0, y0, &bar);
+            if (want_wave) tma_load_2d(sm + F_OM * BOX, &M.om, x0, y0, &bar);
+            tma_load_2d(sm + F_ZCX * BOX, &M.zcx, x0, y0, &bar);
+            tma_load_2d(sm + F_ZCY * BOX, &M.zcy, x0, y0, &bar);
+            tma_load_2d(sm + SM_M, &M.mx[p], x0 + 4, y0 + 2, &bar);
+            tma_load_2d(sm + SM_M + TILE2, &M.my[p], x0 + 4, y0 + 2, &bar);
+            for (int f = 0; f < 12; ++f) bulk_load(sm + SM_ST + f * TILE2, statics[f] + (size_t)t * TILE2, TILE2 * 4, &bar);
+        }
+        const bool ok = mbar_wait(&bar, phase);
+        phase ^= 1u;
+        if (__syncthreads_or(!ok)) {
+            // the copies did not land: report, give them one more bounded wait, and leave the loop
+            if (tid == 0) atomicExch(&ctl->status, W2B_ETIMEOUT);
+            mbar_wait(&bar, phase ^ 1u);
+            return;
+        }
         const int base = (tj * TILE + GY) * A.px + ti * TILE + GX;
         float wmax = 0.0f;
 #pragma unroll 1
-        for (int c = 0; c < 4; ++c) {
-            const int jj = threadIdx.y * 4 + c;
-            const int ii = threadIdx.x;
-            const int k = base + jj * A.px + ii;
+        for (int c = 0; c < 2; ++c) {
+            const int jj = warp + 16 * c, ii = lane;
             const int local = jj * TILE + ii;
-            const int fid = t * TILE2 + local;
-            const float wx = face_step<0>(A, k, fid, t, local, dt, want_wave);
-            const float wy = face_step<1>(A, k, fid, t, local, dt, want_wave);
+            const int b = (jj + 2) * BOXW + ii + 4;
+            const int k = base + jj * A.px + ii;
+            FaceA fx, fy;
+            face_a<0>(sm, b, local, A, t, fx);
+            face_a<1>(sm, b, local, A, t, fy);
+            const float wx = face_bc<0>(sm, b, local, k, A, t, fx, dt, want_wave);
+            const float wy = face_bc<1>(sm, b, local, k, A, t, fy, dt, want_wave);
             wmax = fmax32(wmax, fmax32(wx, wy));
         }
         if (want_wave) {
             const float bm = block_max(wmax, red);
-            if (threadIdx.x == 0 && threadIdx.y == 0) A.wave[t] = bm;
+            if (tid == 0) A.wave[t] = bm;
+        } else {
+            __syncthreads();
         }
     }
     if (!want_wave) return;
     // single-pass grid reduction: the last CTA to finish reduces the per-tile maxima (no CTA waits on another)
-    __shared__ bool last;
-    if (threadIdx.x == 0 && threadIdx.y == 0) {
+    if (tid == 0) {
         __threadfence();
         const unsigned v = atomicAdd(&ctl->ticket, 1u);
         last = (v == gridDim.x - 1);
@@ -226,13 +330,26 @@ __global__ void __launch_bounds__(256) faces_kernel(StepArgs A) {
     if (!last) return;
     __threadfence();
     float w = 0.0f;
-    const int tid = threadIdx.y * blockDim.x + threadIdx.x;
-    for (int a = tid; a < nact; a += blockDim.x * blockDim.y) w = fmax32(w, __ldcg(A.wave + A.active[a]));
+    for (int a = tid; a < nact; a += blockDim.x) w = fmax32(w, __ldcg(A.wave + A.active[a]));
     const float bm = block_max(w, red);
     if (tid == 0) {
         ctl->wave_max = bm;
         ctl->ticket = 0u;
     }
+}
+
+cudaError_t faces_setup() {
+    return cudaFuncSetAttribute(faces_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, FACES_SMEM);
+}
+
+int faces_occupancy() {
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, faces_kernel, FACES_THREADS, FACES_SMEM);
+    return occ;
+}
+
+void launch_faces(const TMaps& M, const StepArgs& A, int p, int grid, cudaStream_t s) {
+    faces_kernel<<<grid, FACES_THREADS, FACES_SMEM, s>>>(M, A, p);
 }
 
 // ------------------------------------------------------------------ update pass

@@ -122,6 +122,11 @@ typedef struct {
 
 int32_t w2b_version(void);
 
+/* Self-check of the step's float cube root (no counterpart in the reference): compares it, over count positive
+ * floats from the bit pattern first_bits on, with the cube root rounded through double, as the reference's float32
+ * cbrt is formed. out (device, 5 uint64, zeroed by the caller): [0] mismatches, [1..4] some mismatching inputs. */
+int32_t w2b_selftest_cbrt(uint32_t first_bits, uint32_t count, uint64_t* out, void* stream);
+
 /* Native layout of a grid. */
 int32_t w2b_layout(const W2BGridDesc* grid, W2BLayout* out);
 

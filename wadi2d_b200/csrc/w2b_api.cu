@@ -13,6 +13,7 @@
 
 namespace w2b {
 cudaError_t faces_setup();
+void launch_cbrt_check(uint32_t first, uint32_t count, unsigned long long* out, cudaStream_t s);
 int faces_occupancy();
 void launch_faces(const TMaps& M, const StepArgs& A, int p, int grid, cudaStream_t s);
 __global__ void update_kernel(StepArgs A);
@@ -230,6 +231,13 @@ using namespace w2b;
 extern "C" {
 
 int32_t w2b_version(void) { return 1; }
+
+int32_t w2b_selftest_cbrt(uint32_t first_bits, uint32_t count, uint64_t* out, void* stream) {
+    if (!out) return W2B_EINVAL;
+    launch_cbrt_check(first_bits, count, reinterpret_cast<unsigned long long*>(out), (cudaStream_t)stream);
+    CKL("w2b_selftest_cbrt");
+    return W2B_OK;
+}
 
 int32_t w2b_layout(const W2BGridDesc* grid, W2BLayout* out) {
     if (!grid || !out || grid->ny <= 0 || grid->nx <= 0 || grid->ny % TILE || grid->nx % TILE || grid->ntiles < 1)

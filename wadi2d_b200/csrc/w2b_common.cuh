@@ -113,8 +113,31 @@ struct TMaps {
 
 // ------------------------------------------------------------------ float32 helpers
 
-// Numba's float32 cbrt is float(cbrt(double(x))); this is the same composition with CUDA's double cbrt.
-__device__ __forceinline__ float cbrt32(float x) { return (float)cbrt((double)x); }
+// x > m^3 for a midpoint m between two adjacent floats, decided exactly. m has a 25-bit significand, so m * m is
+// exact in double and m^3 = p + e exactly with p = fl(m^2 m) and e = fma(m^2, m, -p); x lies within a factor two of
+// p, so x - p is exact (Sterbenz) and x > m^3 exactly when x - p > e.
+__device__ __forceinline__ bool cube_above(double m, float x) {
+    const double m2 = m * m;
+    const double p = m2 * m;
+    const double e = fma(m2, m, -p);
+    return (double)x - p > e;
+}
+
+// The float nearest the cube root of x. Numba's float32 cbrt is float(cbrt(double(x))), the cube root rounded
+// once to double and once to float; this returns the correctly rounded float, which is the same number whenever
+// the double root is within the distance of cbrt(x) from the nearest float midpoint (w2b_selftest_cbrt compares the
+// two over every positive float). Method: cbrtf gives a float within one ulp; of it and its two neighbours the
+// answer is decided by comparing x with the cubes of the two midpoints (cube_above). No midpoint's cube is a float
+// (a 25-bit odd significand cubes to more than 72 bits), so the comparison never ties.
+__device__ __forceinline__ float cbrt32(float x) {
+    if (!(x > 0.0f) || x > 3.0e38f) return (float)cbrt((double)x);  // zero, negative, NaN, huge: the double path
+    const float y = cbrtf(x);
+    const float yu = __int_as_float(__float_as_int(y) + 1);
+    const float yd = __int_as_float(__float_as_int(y) - 1);
+    if (cube_above(0.5 * ((double)y + (double)yu), x)) return yu;
+    if (!cube_above(0.5 * ((double)yd + (double)y), x)) return yd;
+    return y;
+}
 // Python max/min on two ordered floats (the first argument wins a tie).
 __device__ __forceinline__ float fmax32(float a, float b) { return a >= b ? a : b; }
 __device__ __forceinline__ float fmin32(float a, float b) { return a <= b ? a : b; }
@@ -124,6 +147,7 @@ __device__ __forceinline__ float minmod(float a, float b) {
     return fabsf(a) < fabsf(b) ? a : b;
 }
 
+// Velocity at a cell centre from its upwind face uc, with a limited second-order correction (common.cuh:30-34).
 __device__ __forceinline__ float ustar(float uc, float uup, float udown, int second) {
     if (!second) return uc;
     return uc + 0.5f * minmod(uc - uup, udown - uc);

@@ -79,7 +79,7 @@ __device__ __forceinline__ void face_a(const float* sm, int b, int local, const 
 // outputs and wave speed (faces.cu:43-44, :52-63, :102-145). Returns the wave speed.
 template <int AX>
 __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int k, const StepArgs& A, int t,
-                                         const FaceA& F, float dt, int want_wave) {
+                                         const FaceA& F, float dt, int want_wave, const float* rowc) {
     constexpr int S = AX == 0 ? 1 : BOXW;
     constexpr int PP = AX == 0 ? BOXW : 1;
     const W2BParams& P = A.P;
@@ -125,8 +125,10 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
     const float qk = Q[b];
     const float qc_l = HALF * (Q[b - S] + qk);
     const float qc_r = HALF * (qk + Q[b + S]);
-    const float s_l = qc_l > ZERO ? ustar(um, umm, uf, second) : ustar(uf, up, um, second);
-    const float s_r = qc_r > ZERO ? ustar(uf, um, up, second) : ustar(up, upp, uf, second);
+    // each upwind choice picks the arguments of one ustar (the same value as choosing between two ustar calls)
+    const bool pl = qc_l > ZERO, pr = qc_r > ZERO;
+    const float s_l = ustar(pl ? um : uf, pl ? umm : up, pl ? uf : um, second);
+    const float s_r = ustar(pr ? uf : up, pr ? um : upp, pr ? up : uf, second);
     float flux = qc_r * s_r - qc_l * s_l;
     const float qy_s = HALF * (QP[b - S] + QP[b]);
     const float qy_n = HALF * (QP[b - S + PP] + QP[b + PP]);
@@ -134,8 +136,9 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
     const float u_n = gated(U[b + PP], uf, mirror);
     const float uss = gated(U[b - 2 * PP], u_s, mirror);
     const float unn = gated(U[b + 2 * PP], u_n, mirror);
-    const float us_s = qy_s > ZERO ? ustar(u_s, uss, uf, second) : ustar(uf, u_n, u_s, second);
-    const float us_n = qy_n > ZERO ? ustar(uf, u_s, u_n, second) : ustar(u_n, unn, uf, second);
+    const bool ps = qy_s > ZERO, pn = qy_n > ZERO;
+    const float us_s = ustar(ps ? u_s : uf, ps ? uss : u_n, ps ? uf : u_s, second);
+    const float us_n = ustar(pn ? uf : u_n, pn ? u_s : unn, pn ? u_n : uf, second);
     flux += qy_n * us_n - qy_s * us_s;
     // [4] momentum and pressure
     const float abar = HALF * (h_l + h_r) * dx;
@@ -147,23 +150,21 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
         us = uf - press;
     const float vb = 0.25f * (VP[b - S] + VP[b] + VP[b - S + PP] + VP[b + PP]);
 
-    // the table lookup from the quad loaded in part A (common.cuh face_lookup)
+    // the table lookup from the quad loaded in part A (common.cuh face_lookup); rowc holds, per row r, c0^2 and
+    // c1^2 - c0^2 with c0 = r / m, c1 = (r + 1) / m, and in its last slot 1 - c^2 with c = (m - 1) / m: the very
+    // float32 values the lookup forms, computed once a CTA
     const float top = F.top, e = F.eface;
-    const float m = (float)(A.rows - 1);
     const float4 q = F.q;
     float area, tt, w;
     if (F.above) {
         const float a1 = q.z, a0 = q.x;
-        const float c = (m - 1.0f) / m;
-        w = (a1 - a0) / (top * (1.0f - c * c));
+        w = (a1 - a0) / (top * rowc[2 * (A.rows - 1)]);
         area = a1 + w * (e - top);
         tt = q.w * (area / fmax32(a1, 1e-12f));
     } else {
         const int r = F.r;
-        const float c0 = (float)r / m;
-        const float c1 = (float)(r + 1) / m;
-        const float e0 = c0 * c0 * top;
-        const float de = (c1 * c1 - c0 * c0) * top;
+        const float e0 = rowc[2 * r] * top;
+        const float de = rowc[2 * r + 1] * top;
         const float f = (e - e0) / de;
         area = q.x + f * (q.z - q.x);
         tt = q.y + f * (q.w - q.y);
@@ -252,6 +253,7 @@ __global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_co
     extern __shared__ __align__(128) float sm[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ float red[32];
+    __shared__ float rowc[2 * 64 + 1];
     __shared__ bool last;
     Ctl* ctl = A.ctl;
     if (!ctl->run) return;
@@ -262,6 +264,17 @@ __global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_co
     if (tid == 0) {
         mbar_init(&bar, 1);
         fence_barrier_init();
+    }
+    if (tid < A.rows - 1) {
+        const float m = (float)(A.rows - 1);
+        const float c0 = (float)tid / m;
+        const float c1 = (float)(tid + 1) / m;
+        rowc[2 * tid] = c0 * c0;
+        rowc[2 * tid + 1] = c1 * c1 - c0 * c0;
+    } else if (tid == A.rows - 1) {
+        const float m = (float)(A.rows - 1);
+        const float c = (m - 1.0f) / m;
+        rowc[2 * tid] = 1.0f - c * c;
     }
     __syncthreads();
     const uint32_t bytes = (uint32_t)((NBOX - (want_wave ? 0 : 1)) * BOX + 14 * TILE2) * 4u;
@@ -308,8 +321,8 @@ __global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_co
             FaceA fx, fy;
             face_a<0>(sm, b, local, A, t, fx);
             face_a<1>(sm, b, local, A, t, fy);
-            const float wx = face_bc<0>(sm, b, local, k, A, t, fx, dt, want_wave);
-            const float wy = face_bc<1>(sm, b, local, k, A, t, fy, dt, want_wave);
+            const float wx = face_bc<0>(sm, b, local, k, A, t, fx, dt, want_wave, rowc);
+            const float wy = face_bc<1>(sm, b, local, k, A, t, fy, dt, want_wave, rowc);
             wmax = fmax32(wmax, fmax32(wx, wy));
         }
         if (want_wave) {
@@ -336,6 +349,25 @@ __global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_co
         ctl->wave_max = bm;
         ctl->ticket = 0u;
     }
+}
+
+// Every positive float from first (as bits) on: cbrt32 against the double path; out[0] counts mismatches,
+// out[1..4] keep some mismatching inputs.
+__global__ void cbrt_check_kernel(uint32_t first, uint32_t count, unsigned long long* out) {
+    for (uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; n < count; n += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t bits = first + (uint32_t)n;
+        const float x = __uint_as_float(bits);
+        const float a = cbrt32(x);
+        const float b = (float)cbrt((double)x);
+        if (__float_as_uint(a) != __float_as_uint(b) && !(isnan(a) && isnan(b))) {
+            const unsigned long long k = atomicAdd(out, 1ull);
+            if (k < 4) out[1 + k] = bits;
+        }
+    }
+}
+
+void launch_cbrt_check(uint32_t first, uint32_t count, unsigned long long* out, cudaStream_t s) {
+    cbrt_check_kernel<<<148 * 16, 256, 0, s>>>(first, count, out);
 }
 
 cudaError_t faces_setup() {

@@ -229,6 +229,21 @@ int64_t w2b_table_workspace_doubles(int32_t nmax, int64_t threads);
  * hydraulic radius when local != 0), centre beds, inverts, closed faces and natural crests, on the GPU. */
 int32_t w2b_build_tables(const W2BTableIn* in, const W2BTableOut* out, void* stream);
 
+/* w2b_build_tables for callers that cannot allocate device memory. It has no counterpart in the reference. A
+ * library embedded in a host program whose device memory belongs to someone else (a pool or caching allocator it
+ * does not control, a memory cap, an FFI binding with no allocator of its own) still passes its inputs and outputs,
+ * but has no way to hand over the builder's scratch; this entry point allocates nothing (no cudaMalloc, cudaFree or
+ * allocating library call) and uses instead a 32 MiB array of file-scope device memory, which every GPU that loads
+ * the library holds until the process exits. out->ws and out->ws_threads are ignored.
+ *  - Limit: a face's line (k + 2 margin pixels) of at most 3,639 pixels; longer lines are refused with W2B_EINVAL
+ *    and a message. Fewer threads fit the fixed scratch than the caller-scratch entry point uses, so it is slower.
+ *  - The first call on a device looks the array's address up (cudaGetSymbolAddress) with that device current;
+ *    make that first call before any stream capture.
+ *  - Every call shares the one array and it keeps the last call's contents; the kernels write every scratch slot
+ *    before reading it, so nothing has to start at zero. Calls that overlap on the GPU (two streams, two threads)
+ *    race on it: serialise them. */
+int32_t w2b_build_tables_noalloc(const W2BTableIn* in, const W2BTableOut* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -10,6 +10,7 @@
 // ArrayBed hold (wadi2d/tables/builder.py:47-50): a window that reaches past the bed repeats its edge pixel.
 #include <cmath>
 #include <cstdio>
+#include <mutex>
 
 #include "w2b_common.cuh"
 
@@ -519,3 +520,60 @@ int32_t w2b_build_tables(const W2BTableIn* in, const W2BTableOut* out, void* str
 }
 
 }  // extern "C"
+
+// ------------------------------------------------------------------ the table build without allocation
+
+// Scratch of w2b_build_tables_noalloc: 32 MiB of file-scope device memory. Every GPU on which a process loads this
+// library holds it until the process exits, whether the entry point is called or not.
+constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)32 << 20;
+static __device__ __align__(256) double noalloc_scratch[NOALLOC_SCRATCH_BYTES / sizeof(double)];
+
+// The array's device address, looked up once per device with that device current. In host code the name
+// noalloc_scratch is a host-side stand-in, not a device address: a kernel given it would fault or read the wrong
+// memory, so only this address is ever passed on.
+static std::mutex noalloc_mutex;
+static void* noalloc_address[256];
+
+static int noalloc_scratch_address(void** out) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 256) return W2B_ECUDA;
+    std::lock_guard<std::mutex> lock(noalloc_mutex);
+    if (!noalloc_address[dev]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            fprintf(stderr, "libwadi_b200: w2b_build_tables_noalloc: cudaGetSymbolAddress: %s\n",
+                    cudaGetErrorString(e));
+            return W2B_ECUDA;
+        }
+        noalloc_address[dev] = p;
+    }
+    *out = noalloc_address[dev];
+    return W2B_OK;
+}
+
+extern "C" int32_t w2b_build_tables_noalloc(const W2BTableIn* in, const W2BTableOut* out, void* stream) {
+    if (!in || !out) return W2B_EINVAL;
+    W2BTableOut o = *out;
+    o.ws = nullptr;
+    o.ws_threads = 0;
+    if (in->local) {
+        const int margin = in->margin > 0 ? in->margin : 0;
+        const int64_t per_thread = 9 * (int64_t)(in->k + 2 * margin + 1) * (int64_t)sizeof(double);
+        const int64_t threads = (int64_t)(NOALLOC_SCRATCH_BYTES / (size_t)per_thread) / 128 * 128;
+        if (threads < 128) {
+            fprintf(stderr,
+                    "libwadi_b200: w2b_build_tables_noalloc: face lines of %d pixels need %lld bytes of scratch for "
+                    "128 threads; the static scratch holds %zu (at most %lld pixels a line)\n",
+                    in->k + 2 * margin, (long long)(per_thread * 128), NOALLOC_SCRATCH_BYTES,
+                    (long long)(NOALLOC_SCRATCH_BYTES / (128 * 9 * sizeof(double)) - 1));
+            return W2B_EINVAL;
+        }
+        void* ws = nullptr;
+        const int st = noalloc_scratch_address(&ws);
+        if (st != W2B_OK) return st;
+        o.ws = static_cast<double*>(ws);
+        o.ws_threads = threads;
+    }
+    return w2b_build_tables(in, &o, stream);
+}

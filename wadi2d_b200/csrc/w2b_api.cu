@@ -16,7 +16,9 @@ cudaError_t faces_setup();
 void launch_cbrt_check(uint32_t first, uint32_t count, unsigned long long* out, cudaStream_t s);
 int faces_occupancy();
 void launch_faces(const TMaps& M, const StepArgs& A, int p, int grid, cudaStream_t s);
-__global__ void update_kernel(StepArgs A);
+cudaError_t update_setup();
+int update_occupancy();
+void launch_update(const TMaps& M, const StepArgs& A, int p, int grid, cudaStream_t s);
 __global__ void boundary_kernel(StepArgs A, int control);
 __global__ void prestep_kernel(Ctl* ctl);
 __global__ void setstep_kernel(Ctl* ctl, float dtf, int want_wave, int want_wet, int nact);
@@ -190,6 +192,10 @@ static int build_tmaps(Handle& H) {
     box(&H.tmaps.om, B.om);
     box(&H.tmaps.zcx, B.zcx);
     box(&H.tmaps.zcy, B.zcy);
+    box(&H.tmaps.qx1, B.qx1);
+    box(&H.tmaps.qy1, B.qy1);
+    own(&H.tmaps.res, B.res);
+    own(&H.tmaps.src, B.src);
     for (int p = 0; p < 2; ++p) {
         box(&H.tmaps.h[p], B.h[p]);
         box(&H.tmaps.u[p], B.u[p]);
@@ -216,7 +222,7 @@ static int launch_loop_step(Handle& H, int p, cudaStream_t s) {
     const int grid = blocks_for(H, H.g.ntiles - 1);
     prestep_kernel<<<1, 1, 0, s>>>(A.ctl);
     launch_faces(H.tmaps, A, p, faces_grid(H, H.g.ntiles - 1), s);
-    update_kernel<<<grid, blk, 0, s>>>(A);
+    launch_update(H.tmaps, A, p, grid, s);
     boundary_kernel<<<1, 256, 0, s>>>(A, 1);
     activity_kernel<<<1, 1024, 0, s>>>(A);
     plan_kernel<<<grid, blk, 0, s>>>(A, A.woken, -1, A.h_next);
@@ -281,8 +287,11 @@ int32_t w2b_create(const W2BGridDesc* grid, const W2BParams* params, const W2BBu
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&H->sms, cudaDevAttrMultiProcessorCount, dev);
-    int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, update_kernel, 256, 0);
+    if (update_setup() != cudaSuccess) {
+        delete H;
+        return cuda_status(cudaGetLastError(), "w2b_create update_setup");
+    }
+    const int occ = update_occupancy();
     H->step_blocks = H->sms * (occ > 0 ? occ : 1);
     if (faces_setup() != cudaSuccess) {
         delete H;
@@ -385,10 +394,9 @@ int32_t w2b_step(void* handle, float dt, int32_t want_wave, int32_t want_wet, vo
         return W2B_OK;
     }
     const StepArgs A = make_args(*H, H->cur);
-    const dim3 blk(32, 8);
     const int grid = blocks_for(*H, H->nact);
     launch_faces(H->tmaps, A, H->cur, faces_grid(*H, H->nact), s);
-    update_kernel<<<grid, blk, 0, s>>>(A);
+    launch_update(H->tmaps, A, H->cur, grid, s);
     if (H->nb) boundary_kernel<<<1, 256, 0, s>>>(A, 0);
     CKL("w2b_step");
     H->cur ^= 1;
@@ -405,12 +413,11 @@ int32_t w2b_step_timed(void* handle, float dt, int32_t want_wave, int32_t want_w
     if (want_wave) CK(cudaMemsetAsync(H->B.wave, 0, sizeof(float) * H->g.ntiles, s));
     setstep_kernel<<<1, 1, 0, s>>>(H->ctl(), dt, want_wave, want_wet, H->nact);
     const StepArgs A = make_args(*H, H->cur);
-    const dim3 blk(32, 8);
     const int grid = blocks_for(*H, H->nact);
     CK(cudaEventRecord(ev[0], s));
     launch_faces(H->tmaps, A, H->cur, faces_grid(*H, H->nact), s);
     CK(cudaEventRecord(ev[1], s));
-    update_kernel<<<grid, blk, 0, s>>>(A);
+    launch_update(H->tmaps, A, H->cur, grid, s);
     CK(cudaEventRecord(ev[2], s));
     if (H->nb) boundary_kernel<<<1, 256, 0, s>>>(A, 0);
     CK(cudaEventRecord(ev[3], s));

@@ -109,6 +109,8 @@ struct StepArgs {
 // momenta, which the face pass reads at own faces only. Ping-pong pairs have one map a half.
 struct TMaps {
     CUtensorMap d, h[2], u[2], v[2], qx, qy, om, zcx, zcy, mx[2], my[2];
+    CUtensorMap qx1, qy1;  // 40 x 36 boxes for the update pass
+    CUtensorMap res, src;  // 32 x 32 boxes
 };
 
 // ------------------------------------------------------------------ float32 helpers

@@ -413,8 +413,20 @@ __device__ __forceinline__ void envelope(const StepArgs& A, int fid, int k, floa
 
 constexpr int RING = TILE + 2;  // the tile and its one-cell ring
 constexpr int RPAD = RING + 1;
+constexpr int U_QX1 = 0, U_QY1 = 1, U_H = 2;       // 40 x 36 boxes
+constexpr int U_OWN = 3 * BOX;                      // res, src, hc: 32 x 32 each
+constexpr int U_R = U_OWN + 3 * TILE2;              // r of the tile and its ring
+constexpr int U_FLOATS = U_R + RING * RPAD;
+constexpr int UPDATE_SMEM = U_FLOATS * 4;           // 34,328 bytes
+constexpr int UPDATE_THREADS = 256;
 
-__global__ void __launch_bounds__(256) update_kernel(StepArgs A) {
+// The update pass (wadi2d/solver/gpu/kernels/cells.cu:4-63 with limit fused in): TMA stages the tile's unscaled
+// discharges and old depth with their ring, its residual, source and Hc; r of the tile and its one-cell ring is
+// formed in shared memory; then each thread takes its four cells through continuity, issues their four level-table
+// loads together, and finishes the level, the wet share, the wet flag and, on envelope steps, the envelope.
+__global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_constant__ TMaps M, StepArgs A, int p) {
+    extern __shared__ __align__(128) float sm[];
+    __shared__ __align__(8) uint64_t bar;
     Ctl* ctl = A.ctl;
     if (!ctl->run) return;
     const int nact = ctl->nact;
@@ -425,53 +437,127 @@ __global__ void __launch_bounds__(256) update_kernel(StepArgs A) {
     const float time = ctl->max_time, arrive = ctl->arrive, deep = ctl->deep;
     const float area = A.area;
     const int px = A.px;
-    const float* __restrict__ q1x = A.q1[0];
-    const float* __restrict__ q1y = A.q1[1];
-    __shared__ float rs[RING * RPAD];
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    const int rows = A.rows, last = rows - 1;
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        fence_barrier_init();
+    }
+    __syncthreads();
+    const uint32_t bytes = (uint32_t)(3 * BOX + 3 * TILE2) * 4u;
+    uint32_t phase = 0;
+    const float* QX1 = sm + U_QX1 * BOX;
+    const float* QY1 = sm + U_QY1 * BOX;
+    const float* H = sm + U_H * BOX;
+    const float* RES = sm + U_OWN;
+    const float* SRC = sm + U_OWN + TILE2;
+    const float* HC = sm + U_OWN + 2 * TILE2;
+    float* rs = sm + U_R;
     for (int a = blockIdx.x; a < nact; a += gridDim.x) {
         const int t = A.active[a];
         const int tj = A.tiles[2 * t], ti = A.tiles[2 * t + 1];
-        const int base = (tj * TILE + GY) * px + ti * TILE + GX;
-        // positivity ratio r of the tile and its ring (wadi2d/solver/gpu/kernels/cells.cu:4-19), from the old h
-        for (int idx = tid; idx < RING * RING; idx += 256) {
+        if (tid == 0) {
+            fence_proxy_async();
+            mbar_expect_tx(&bar, bytes);
+            const int x0 = ti * TILE + GX - 4, y0 = tj * TILE + GY - 2;
+            tma_load_2d(sm + U_QX1 * BOX, &M.qx1, x0, y0, &bar);
+            tma_load_2d(sm + U_QY1 * BOX, &M.qy1, x0, y0, &bar);
+            tma_load_2d(sm + U_H * BOX, &M.h[p], x0, y0, &bar);
+            tma_load_2d(sm + U_OWN, &M.res, x0 + 4, y0 + 2, &bar);
+            tma_load_2d(sm + U_OWN + TILE2, &M.src, x0 + 4, y0 + 2, &bar);
+            bulk_load(sm + U_OWN + 2 * TILE2, A.hc + (size_t)t * TILE2, TILE2 * 4, &bar);
+        }
+        const bool ok = mbar_wait(&bar, phase);
+        phase ^= 1u;
+        if (__syncthreads_or(!ok)) {
+            if (tid == 0) atomicExch(&ctl->status, W2B_ETIMEOUT);
+            mbar_wait(&bar, phase ^ 1u);
+            return;
+        }
+        // positivity ratio r (wadi2d/solver/gpu/kernels/cells.cu:4-19) of the tile and its ring, from the old h
+        for (int idx = tid; idx < RING * RING; idx += UPDATE_THREADS) {
             const int rj = idx / RING, ri = idx - rj * RING;
-            const int k = base + (rj - 1) * px + (ri - 1);
-            const float out = fmax32(__ldg(q1x + k + 1), 0.0f) + fmax32(-__ldg(q1x + k), 0.0f) +
-                              fmax32(__ldg(q1y + k + px), 0.0f) + fmax32(-__ldg(q1y + k), 0.0f);
-            const float have = fmax32(__ldg(A.h + k), 0.0f) * area;
+            const int b = (rj + 1) * BOXW + ri + 3;  // cell (rj - 1, ri - 1)
+            const float out = fmax32(QX1[b + 1], 0.0f) + fmax32(-QX1[b], 0.0f) + fmax32(QY1[b + BOXW], 0.0f) +
+                              fmax32(-QY1[b], 0.0f);
+            const float have = fmax32(H[b], 0.0f) * area;
             rs[rj * RPAD + ri] = out * dt > have ? have / (out * dt) : 1.0f;
         }
         __syncthreads();
-        int any = 0;
-        const float2* __restrict__ pairs_t = A.dtab2 + (size_t)t * (A.rows - 1) * TILE2;
-#pragma unroll 1
+        const int base = (tj * TILE + GY) * px + ti * TILE + GX;
+        const float2* __restrict__ pairs_t = A.dtab2 + (size_t)t * (rows - 1) * TILE2;
+        // continuity (cells.cu:219-232) for the thread's four cells
+        float hn[4], sv[4];
+        int rr[4];
+#pragma unroll
         for (int c = 0; c < 4; ++c) {
-            const int jj = threadIdx.y * 4 + c;
-            const int ii = threadIdx.x;
-            const int k = base + jj * px + ii;
+            const int jj = threadIdx.y * 4 + c, ii = threadIdx.x;
             const int local = jj * TILE + ii;
-            const int fid = t * TILE2 + local;
+            const int b = (jj + 2) * BOXW + ii + 4;
+            const int k = base + jj * px + ii;
             const float* row = rs + (jj + 1) * RPAD + (ii + 1);
             const float rc = row[0];
-            const float qw = scaled(__ldg(q1x + k), row[-1], rc);
-            const float qe = scaled(__ldg(q1x + k + 1), rc, row[1]);
-            const float qn = scaled(__ldg(q1y + k), row[-RPAD], rc);
-            const float qs = scaled(__ldg(q1y + k + px), rc, row[RPAD]);
+            const float qw = scaled(QX1[b], row[-1], rc);
+            const float qe = scaled(QX1[b + 1], rc, row[1]);
+            const float qn = scaled(QY1[b], row[-RPAD], rc);
+            const float qs = scaled(QY1[b + BOXW], rc, row[RPAD]);
             A.q[0][k] = qw;
             A.q[1][k] = qn;
-            const float h0 = __ldg(A.h + k);
-            const float inc = A.res[k] + dt * __ldg(A.src + k) - dt * (qe - qw + qs - qn) / area;
+            const float h0 = H[b];
+            const float inc = RES[local] + dt * SRC[local] - dt * (qe - qw + qs - qn) / area;
             const float total = h0 + inc;
-            const float hn = fmax32(total, 0.0f);
+            hn[c] = fmax32(total, 0.0f);
             A.res[k] = total > 0.0f ? inc - (total - h0) : 0.0f;
-            A.h_next[k] = hn;
-            const float hcv = __ldg(A.hc + fid);
-            const float dk = cell_level(hn, hcv, pairs_t + local, A.rows, A.P.level_fp64);
+            A.h_next[k] = hn[c];
+            // the level table's row (common.cuh cell_level): the top row above Hc, none where Hc <= 0
+            const float hcv = HC[local];
+            if (hcv <= 0.0f) {
+                rr[c] = -1;
+                sv[c] = 0.0f;
+            } else if (hn[c] >= hcv) {
+                rr[c] = last - 1;
+                sv[c] = -1.0f;
+            } else {
+                sv[c] = sqrtf(hn[c] / hcv) * (float)last;
+                rr[c] = row_of(sv[c], last);
+            }
+        }
+        float2 pr[4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int local = (threadIdx.y * 4 + c) * TILE + threadIdx.x;
+            pr[c] = rr[c] >= 0 ? __ldg(pairs_t + (size_t)rr[c] * TILE2 + local) : make_float2(0.0f, 0.0f);
+        }
+        int any = 0;
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int jj = threadIdx.y * 4 + c, ii = threadIdx.x;
+            const int local = jj * TILE + ii;
+            const int k = base + jj * px + ii;
+            const float hcv = HC[local];
+            const float h = hn[c];
+            float dk, om = 1.0f;
+            if (hcv <= 0.0f) {
+                dk = h;
+            } else if (h >= hcv) {
+                dk = pr[c].y + (h - hcv);
+            } else {
+                const int r = rr[c];
+                const float2 q = pr[c];
+                if (A.P.level_fp64 && r == 0) {
+                    const double sd = sqrt((double)h / (double)hcv) * (double)last;
+                    dk = (float)((double)q.x + sd * ((double)q.y - (double)q.x));
+                } else {
+                    dk = q.x + (sv[c] - (float)r) * (q.y - q.x);
+                }
+                const float m = (float)last;
+                om = hcv * (float)(2 * r + 1) / (m * m) / fmax32(q.y - q.x, 1e-12f);
+            }
             A.d[k] = dk;
-            if (want_plan) A.om[k] = cell_plan(hn, hcv, pairs_t + local, A.rows);
-            any |= hn > 0.0f;
-            if (want_max && !((A.bmark[t * TILE + jj] >> ii) & 1u)) envelope(A, fid, k, dk, hn, time, arrive, deep);
+            if (want_plan) A.om[k] = om;
+            any |= h > 0.0f;
+            if (want_max && !((A.bmark[t * TILE + jj] >> ii) & 1u))
+                envelope(A, t * TILE2 + local, k, dk, h, time, arrive, deep);
         }
         if (want_wet) {
             const int w = __syncthreads_or(any);
@@ -480,6 +566,20 @@ __global__ void __launch_bounds__(256) update_kernel(StepArgs A) {
             __syncthreads();
         }
     }
+}
+
+cudaError_t update_setup() {
+    return cudaFuncSetAttribute(update_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, UPDATE_SMEM);
+}
+
+int update_occupancy() {
+    int occ = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, update_kernel, UPDATE_THREADS, UPDATE_SMEM);
+    return occ;
+}
+
+void launch_update(const TMaps& M, const StepArgs& A, int p, int grid, cudaStream_t s) {
+    update_kernel<<<grid, dim3(32, 8), UPDATE_SMEM, s>>>(M, A, p);
 }
 
 // ------------------------------------------------------------------ boundary, tally, control (one CTA)

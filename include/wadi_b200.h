@@ -192,6 +192,35 @@ int32_t w2b_tally(void* handle, double dt, void* stream);
 int32_t w2b_advance(void* handle, const W2BStepper* cfg, double t_end, int64_t max_steps, W2BClock* clock,
                     void* stream);
 
+/* Rain of a source window on the device (the device form of wadi2d/forcing.py:667-683, the SCS loss of
+ * wadi2d/hydrology/losses.py:69-72, and an initial-and-constant loss with no counterpart on the reference's grid
+ * cells). Per rained cell m (NATIVE index cells[m]): cumulative rain P = depth[m] * f at the window's start (f0) and
+ * end (f1), mm; loss 0 none, 1 SCS (s_mm, ia_mm per cell), 2 initial ia_mm then fc_mm_h; src = excess / (1000 dt).
+ * partial: W2B_PARTIALS doubles of scratch. */
+#define W2B_PARTIALS 296
+typedef struct {
+    int64_t n;
+    const int32_t* cells;
+    const double* depth;
+    int32_t loss;
+    const double* s_mm;
+    const double* ia_mm;
+    double fc_mm_h;
+    double* partial;
+} W2BRain;
+
+/* The cell size the handle's kernels use (W2BParams.dx). */
+int32_t w2b_cell_size(void* handle, float* dx);
+
+/* Replaces Forcing.rate's rain part (wadi2d/forcing.py:667-683) for a window [t0, t1]: writes src at the rained cells
+ * and volume[0] (device) = the window's rain volume, m3 (float32 rates summed in FP64, times dx^2 (t1 - t0)). */
+int32_t w2b_rain_window(void* handle, const W2BRain* rain, double f0, double f1, double t0, double t1,
+                        double* volume, void* stream);
+
+/* Replaces Monitor.storage (wadi2d/engine/monitor.py:214-218): out[0] (device) = dx^2 * sum of h + res over the n
+ * NATIVE cells, FP64. partial: W2B_PARTIALS doubles of scratch. */
+int32_t w2b_storage(void* handle, int64_t n, const int32_t* cells, double* partial, double* out, void* stream);
+
 /* Inputs of the table builder (wadi2d/tables/builder.py:131-258; kernels of wadi2d/tables/core.py). Device pointers.
  * (ny, nx) grids are row-major float64, except mask and walls (uint8, 1 = set). Pixel (r, c) of the grid origin is
  * z[(r + row_offset) * zw + c + col_offset], indices clipped to the bed as an ArrayBed window is

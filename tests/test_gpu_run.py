@@ -1,0 +1,122 @@
+"""Runs on the B200: the device rain and storage against the host forms, and configuration 1 at full size
+(256 x 256 cells, 2 h, CFL 0.9, 1 h of rain) against the oracle field by field, with the mass balance."""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from wadi2d_b200 import forcing as F
+from wadi2d_b200 import workloads
+from wadi2d_b200.backend import BoundaryCells
+from wadi2d_b200.config import Numerics
+from wadi2d_b200.grid import TileGrid
+from wadi2d_b200.maxima import Tally
+from wadi2d_b200.model import Model
+from wadi2d_b200.run import DeviceRain, DeviceStorage, run_windows
+from wadi2d_b200.state import from_state, state_index
+from wadi2d_b200.tables import GridTables
+
+pytestmark = pytest.mark.gpu
+
+
+def c1(n: int):
+    w = workloads.v_channel_plane(n=n, dx=10.0, k=5, seed=0)
+    og = O.Grid.from_mask(np.ones((n, n), bool), 0.0, 0.0, w.dx)
+    tab = O.build_tables(og, w.z, w.dx / w.k, w.manning)
+    g = TileGrid.from_mask(np.ones((n, n), bool), 0.0, 0.0, w.dx)
+    return w, og, g, tab
+
+
+@pytest.mark.parametrize("loss", ["none", "scs", "ic"])
+def test_device_rain_equals_host_rate(loss):
+    w, og, g, tab = c1(64)
+    m = Model(GridTables.from_dict(g, tab), Numerics())
+    jj, ii = np.nonzero(g.mask)
+    cells = state_index(g, jj, ii).astype(np.int64)
+    rng = np.random.default_rng(4)
+    mult = rng.lognormal(0.0, 0.4, cells.size)
+    storm = F.TriangularStorm(80.0, 180.0)
+    cn = rng.choice([60.0, 75.0, 90.0], cells.size)
+    lossobj = {"none": None, "scs": F.ScsCurveNumber(cn), "ic": F.InitialConstantLoss(10.0, 2.0)}[loss]
+    host = F.Forcing(cells, w.dx**2, storm, depth_factor=mult, loss=lossobj,
+                     class_of=np.arange(cells.size) if loss == "scs" else None)  # fmt: skip
+    dev = DeviceRain(m, storm, cells, multiplier=mult, loss=lossobj, curve_number=cn if loss == "scs" else None)
+    for t0, t1 in ((0.0, 30.0), (1200.0, 1230.0), (5390.0, 5420.0), (10780.0, 10810.0)):
+        rate, rain, _ = host.rate(t0, t1)
+        vol = dev.window(t0, t1)
+        got = m.backend.src[cells]
+        assert np.array_equal(got, rate), (loss, t0)
+        assert vol == pytest.approx(rain, rel=1e-12, abs=1e-9)
+
+
+def test_device_storage_equals_host_sum():
+    w, og, g, tab = c1(64)
+    m = Model(GridTables.from_dict(g, tab), Numerics())
+    rng = np.random.default_rng(2)
+    m.set_depth(np.where(g.mask, rng.random(g.shape) * 0.3, 0.0))
+    jj, ii = np.nonzero(g.mask)
+    cells = state_index(g, jj, ii).astype(np.int64)
+    assert DeviceStorage(m, cells)() == pytest.approx(F.storage(m, cells), rel=1e-13)
+
+
+def _drive(m, g, w, rain_rate, outfall, t_mid, t_end, device):
+    """Rain for t_mid seconds, then none, to t_end; the outfall tally and books either on the device or the host."""
+    rate = np.zeros(g.shape)
+    rate[1 : 1 + w.ny, 1 : w.nx] = rain_rate
+    m.set_source(rate)
+    if device:
+        tally = Tally(m, outfall.astype(np.int64), np.ones(outfall.size), np.zeros(0, np.int64), np.zeros(0))
+        m.run(t_mid, tally=tally)
+        m.set_source(np.zeros(g.shape))
+        m.run(t_end, tally=tally)
+        return tally.volume()
+    tally = O.Tally(m, outfall, np.ones(outfall.size), np.zeros(0, np.int64), np.zeros(0))
+    last = [0.0]
+
+    def on_step(st):
+        tally.add(st.t - last[0])
+        last[0] = st.t
+
+    m.advance(t_mid, on_step)
+    m.set_source(np.zeros(g.shape))
+    m.advance(t_end, on_step)
+    return tally.volume()
+
+
+def test_configuration1_full_size_matches_the_oracle_and_balances():
+    n = 256
+    w, og, g, tab = c1(n)
+    O.threads(0)
+    rows, cols = w.outfall
+    out_ref = np.array([state_index(g, int(j), int(i)) for j, i in zip(rows, cols, strict=True)], np.int32)
+    nb = out_ref.size
+    bc = (out_ref, np.zeros(nb, np.int32), np.ones(nb, np.int32), np.zeros(nb, np.float32), np.zeros(nb, np.float32))
+    rain_rate = w.rain_mm_h / 3.6e6
+    om = O.Model(og, tab, O.Numerics(cfl=w.cfl))
+    om.set_boundary(O.Boundary(*bc))
+    out_o = _drive(om, og, w, rain_rate, out_ref, w.rain_s, w.t_end, device=False)
+    m = Model(GridTables.from_dict(g, tab), Numerics(cfl=w.cfl))
+    m.set_boundary(BoundaryCells(*bc))
+    out_g = _drive(m, g, w, rain_rate, out_ref, w.rain_s, w.t_end, device=True)
+    assert m.stepper.nsteps == om.nsteps
+    for name in ("h", "d", "qx", "qy", "u", "v"):
+        a, b = m.field(name), O.from_state(og, om.backend.get_field(name))
+        scale = max(float(np.abs(b).max()), 1e-6)
+        tol = 1e-5 if name in ("h", "d") else 1e-4 * scale
+        assert np.abs(a - b).max() <= tol, name
+    assert np.array_equal(m.field("h") > 0, O.from_state(og, om.backend.get_field("h")) > 0)
+    assert out_g == pytest.approx(out_o, rel=1e-9)
+    # the books: rain in = outflow + storage change (interior cells), FP64
+    taken = np.zeros(g.shape, bool)
+    taken[rows, cols] = True
+    jj, ii = np.nonzero(g.mask & ~taken)
+    interior = state_index(g, jj, ii).astype(np.int64)
+    area = w.dx**2
+    rained = np.zeros(g.shape, bool)
+    rained[1 : 1 + w.ny, 1 : w.nx] = True
+    cells_rained = int((rained & g.mask & ~taken).sum())
+    rain_volume = float(np.float32(rain_rate)) * cells_rained * area * w.rain_s
+    bal = F.Balance(rain=rain_volume, outflow=out_g, storage=F.storage(m, interior))
+    assert abs(bal.relative) < 1e-6, bal

@@ -59,6 +59,14 @@ class Stepper(ctypes.Structure):
     ] + [("arrive", c_f32), ("deep", c_f32)]
 
 
+class Rain(ctypes.Structure):
+    _fields_ = [("n", c_i64), ("cells", c_vp), ("depth", c_vp), ("loss", c_i32), ("s_mm", c_vp), ("ia_mm", c_vp),
+                ("fc_mm_h", c_f64), ("partial", c_vp)]  # fmt: skip
+
+
+PARTIALS = 296
+
+
 class Clock(ctypes.Structure):
     _fields_ = [("t", c_f64), ("dt", c_f64), ("nsteps", c_i64), ("refresh_due", c_i32), ("status", c_i32),
                 ("wave_max", c_f32), ("nact", c_i32)]  # fmt: skip
@@ -88,6 +96,9 @@ _SIGNATURES = {
     "w2b_tally": [c_vp, c_f64, c_vp],
     "w2b_advance": [c_vp, ctypes.POINTER(Stepper), c_f64, c_i64, ctypes.POINTER(Clock), c_vp],
     "w2b_build_tables": [c_vp, c_vp, c_vp],
+    "w2b_cell_size": [c_vp, ctypes.POINTER(c_f32)],
+    "w2b_rain_window": [c_vp, c_vp, c_f64, c_f64, c_f64, c_f64, c_vp, c_vp],
+    "w2b_storage": [c_vp, c_i64, c_vp, c_vp, c_vp, c_vp],
 }
 
 _lib = None

@@ -483,6 +483,12 @@ static float* field_ptr(Handle* H, int f) {
     }
 }
 
+int32_t w2b_cell_size(void* handle, float* dx) {
+    if (!handle || !dx) return W2B_EINVAL;
+    *dx = static_cast<Handle*>(handle)->P.dx;
+    return W2B_OK;
+}
+
 int32_t w2b_field_ptr(void* handle, int32_t field, float** out) {
     if (!handle || !out) return W2B_EINVAL;
     float* p = field_ptr(static_cast<Handle*>(handle), field);

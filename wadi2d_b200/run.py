@@ -1,0 +1,135 @@
+"""The run driver's window loop (wadi2d/run.py:1712-1740) on the B200 backend: per source window the net source is
+set, the model advances to the window's end on the device (envelope and FP64 outfall tally inside the loop), and the
+books are kept as the reference's monitor keeps them (wadi2d/engine/monitor.py:36-80, :197-218).
+
+Rain comes either from the host (``forcing.Forcing.rate``, the reference's form: a float32 rate per interior cell
+uploaded each window) or from the device (``DeviceRain``: the same rate formed on the GPU from per-cell storm depth
+multipliers, which removes the per-window upload).
+"""
+
+from __future__ import annotations
+
+import ctypes
+from dataclasses import dataclass
+
+import numpy as np
+
+from wadi2d_b200 import _lib
+from wadi2d_b200.forcing import Balance, InitialConstantLoss, ScsCurveNumber
+from wadi2d_b200.layout import native_of_ref
+
+SECONDS_PER_MINUTE = 60.0
+
+
+class DeviceRain:
+    """A storm over a set of cells, rated on the device each window (w2b_rain_window).
+
+    ``cells``: reference state indices of the rained cells; ``multiplier``: per-cell factor on the storm's cumulative
+    depth (a depth grid; 1 for uniform rain); ``loss``: ScsCurveNumber (per-cell curve numbers), InitialConstantLoss,
+    or None."""
+
+    def __init__(self, model, storm, cells, multiplier=None, loss=None, curve_number=None) -> None:
+        b = model.backend
+        torch = b.torch
+        self.model, self.storm = model, storm
+        dev = b.device
+        n = int(np.asarray(cells).size)
+        native = native_of_ref(model.grid.tiles, cells, model.grid.shape[1]).astype(np.int32)
+        self.cells = torch.as_tensor(native, device=dev)
+        mult = np.ones(n) if multiplier is None else np.asarray(multiplier, np.float64)
+        self.depth = torch.as_tensor(mult, dtype=torch.float64, device=dev)
+        self.partial = torch.zeros(_lib.PARTIALS, dtype=torch.float64, device=dev)
+        self.volume = torch.zeros(1, dtype=torch.float64, device=dev)
+        self.s = self.ia = None
+        kind, fc = 0, 0.0
+        if isinstance(loss, ScsCurveNumber):
+            cn = np.broadcast_to(np.asarray(curve_number if curve_number is not None else loss.curve_number,
+                                            np.float64), (n,))  # fmt: skip
+            scs = ScsCurveNumber(cn, loss.initial_abstraction_mm)
+            self.s = torch.as_tensor(np.broadcast_to(scs.retention_mm, (n,)).copy(), device=dev)
+            self.ia = torch.as_tensor(np.broadcast_to(scs.abstraction_mm, (n,)).astype(np.float64).copy(), device=dev)
+            kind = 1
+        elif isinstance(loss, InitialConstantLoss):
+            self.ia = torch.full((n,), float(loss.initial_mm), dtype=torch.float64, device=dev)
+            fc, kind = float(loss.constant_mm_h), 2
+        self.tiles = np.unique(np.asarray(cells, np.int64) // 1296)
+        self.rain = _lib.Rain(n, self.cells.data_ptr(), self.depth.data_ptr(), kind,
+                              None if self.s is None else self.s.data_ptr(),
+                              None if self.ia is None else self.ia.data_ptr(), fc, self.partial.data_ptr())  # fmt: skip
+
+    def window(self, t0: float, t1: float) -> float:
+        """Write the window's rates into src; return its rain volume, m3."""
+        f0 = float(np.asarray(self.storm.cumulative_depth(np.array([t0 / SECONDS_PER_MINUTE])))[0])
+        f1 = float(np.asarray(self.storm.cumulative_depth(np.array([t1 / SECONDS_PER_MINUTE])))[0])
+        b = self.model.backend
+        _lib.call("w2b_rain_window", b.handle, ctypes.byref(self.rain), f0, f1, float(t0), float(t1),
+                  self.volume.data_ptr(), b._stream())  # fmt: skip
+        return float(self.volume.item())
+
+
+class DeviceStorage:
+    """FP64 storage (h + res) over a set of cells, on the device (w2b_storage)."""
+
+    def __init__(self, model, cells) -> None:
+        b = model.backend
+        torch = b.torch
+        self.model = model
+        native = native_of_ref(model.grid.tiles, cells, model.grid.shape[1]).astype(np.int32)
+        self.cells = torch.as_tensor(native, device=b.device)
+        self.partial = torch.zeros(_lib.PARTIALS, dtype=torch.float64, device=b.device)
+        self.out = torch.zeros(1, dtype=torch.float64, device=b.device)
+
+    def __call__(self) -> float:
+        b = self.model.backend
+        _lib.call("w2b_storage", b.handle, int(self.cells.numel()), self.cells.data_ptr(), self.partial.data_ptr(),
+                  self.out.data_ptr(), b._stream())  # fmt: skip
+        return float(self.out.item())
+
+
+@dataclass
+class RunSummary:
+    t: float
+    steps: int
+    windows: int
+    balance: Balance
+
+
+def run_windows(model, t_end: float, rain=None, host_forcing=None, window: float = 30.0, maxima=None, tally=None,
+                storage=None, on_window=None) -> RunSummary:  # fmt: skip
+    """Advance ``model`` to ``t_end`` window by window; rain from ``rain`` (DeviceRain) or ``host_forcing``
+    (forcing.Forcing, whose ``state`` are the interior cells)."""
+    bal = Balance()
+    if storage is not None:
+        bal.storage0 = bal.storage = storage()
+    t = model.stepper.t
+    n0 = model.stepper.nsteps
+    windows = 0
+    while t < t_end - 1e-9:
+        t1 = min(t + window, t_end)
+        if rain is not None:
+            bal.rain += rain.window(t, t1)
+            st = model.stepper
+            if st.adaptive_active:  # as set_source_cells does: rained tiles stay active while rain falls
+                falling = rain.storm.cumulative_depth(np.array([t1 / 60.0]))[0] > rain.storm.cumulative_depth(
+                    np.array([t / 60.0]))[0]
+                st.keep_active[:] = False
+                if falling:
+                    st.keep_active[rain.tiles] = True
+                st.keep_active[model.boundary_tiles] = True
+                st.rebuild_active(retain=True)
+            st.refresh_due = True
+        elif host_forcing is not None:
+            rate, r, q = host_forcing.rate(t, t1)
+            model.set_source_cells(host_forcing.state, rate)
+            bal.rain += r
+            bal.inflow += q
+        model.run(t1, maxima=maxima, tally=tally)
+        t = model.stepper.t
+        windows += 1
+        if on_window is not None:
+            on_window(t, bal)
+    if tally is not None:
+        bal.outflow = tally.volume()
+    if storage is not None:
+        bal.storage = storage()
+    return RunSummary(t, model.stepper.nsteps - n0, windows, bal)

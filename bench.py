@@ -57,6 +57,13 @@ def parse():
     p.add_argument("--e2e-windows", type=int, default=4)
     p.add_argument("--full-run", action="store_true",
                    help="the whole 36 h run of configuration 3 from dry ground, with its mass balance")
+    p.add_argument("--ensemble", action="store_true",
+                   help="configuration 4: the storm sweep as one batch against the same runs one after another")
+    p.add_argument("--runs", type=int, default=64, help="runs of the ensemble")
+    p.add_argument("--side-max", type=int, default=2048, help="largest side of an ensemble run, cells")
+    p.add_argument("--recession-min", type=float, default=30.0, help="simulated time after each storm, minutes")
+    p.add_argument("--time-scale", type=float, default=1.0, help="share of each run's simulated time to step")
+    p.add_argument("--skip-plain", action="store_true", help="the batch only (no one-after-another sweep)")
     return p.parse_args()
 
 
@@ -265,6 +272,108 @@ def full_run(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def ensemble_inputs(spec, dev):
+    """One run of configuration 4 on the GPU: fan, tables, outfalls, tally faces, rained interior cells."""
+    from wadi2d_b200 import forcing as F
+    from wadi2d_b200 import workloads
+    from wadi2d_b200.backend import BoundaryCells
+    from wadi2d_b200.config import Tables
+    from wadi2d_b200.grid import TileGrid
+    from wadi2d_b200.state import state_index
+    from wadi2d_b200.tables import ArrayBed, build_tables
+
+    n = spec.side
+    c = workloads.catchment(n=n, dx=spec.dx, k=4, seed=spec.seed, relief=spec.relief, device=dev)
+    grid = TileGrid.from_mask(np.ones((n, n), bool), 0.0, 0.0, spec.dx)
+    tables = build_tables(grid, ArrayBed(c.z, spec.dx / 4), Tables(), c.manning, device=dev)
+    del c.z
+    rows, cols = c.boundary_cells()
+    cells = state_index(grid, rows, cols).astype(np.int32)
+    nb = cells.size
+    bc = BoundaryCells(cells, cells.copy(), np.ones(nb, np.int32), np.zeros(nb, np.float32), np.zeros(nb, np.float32))
+    taken = np.zeros(grid.shape, bool)
+    taken[rows, cols] = True
+    inner = grid.mask & ~taken
+    jj, ii = np.nonzero(inner)
+    (xf, xs), (yf, ys) = F.open_faces(grid, inner, taken)
+    return grid, tables, bc, state_index(grid, jj, ii).astype(np.int64), (xf, xs, yf, ys)
+
+
+def ensemble_run(args) -> None:
+    """Configuration 4: 64 runs of uneven size, cell size and storm (uniform rain, each run its own depth, duration
+    and ARF factor), each from dry ground to the end of its storm plus a recession, the envelope every 4 steps and
+    the FP64 outfall tally every step. Timed twice on one GPU: as one batch (w2b_advance_runs) and one run after
+    another (the plain per-run device loop). Both give every run the same steps and the same envelope."""
+    import torch
+
+    from wadi2d_b200 import workloads
+    from wadi2d_b200.batch import Batch
+    from wadi2d_b200.config import Numerics
+    from wadi2d_b200.maxima import Maxima, Tally
+    from wadi2d_b200.model import Model
+    from wadi2d_b200.run import DeviceRain, run_windows
+
+    dev = torch.device("cuda", 0)
+    specs = workloads.ensemble(args.runs, side_max=args.side_max)
+    t0 = time.perf_counter()
+    inputs = [ensemble_inputs(sp, dev) for sp in specs]
+    torch.cuda.synchronize(dev)
+    setup = time.perf_counter() - t0
+    num = Numerics()
+    t_end = np.array([(sp.duration_min + args.recession_min) * 60.0 * args.time_scale for sp in specs])
+    storms = [sp.storm() for sp in specs]
+    cells = np.array([int(i[0].mask.sum()) for i in inputs], np.float64)
+    plain = None
+    if not args.skip_plain:
+        steps, peak, walls = [], [], []
+        for r, (grid, tables, bc, interior, tspec) in enumerate(inputs):
+            m = Model(tables, num)
+            m.set_boundary(bc)
+            m.set_depth(np.zeros(grid.shape))
+            tally = Tally(m, *tspec)
+            maxima = Maxima(m, 0.1, 0.05, every=4)
+            rain = DeviceRain(m, storms[r], interior)
+            torch.cuda.synchronize(dev)
+            w0 = time.perf_counter()
+            run_windows(m, t_end[r], rain=rain, window=30.0, maxima=maxima, tally=tally)
+            torch.cuda.synchronize(dev)
+            walls.append(time.perf_counter() - w0)
+            steps.append(m.stepper.nsteps)
+            peak.append(float(maxima.fields()["depth"].max()))
+            del m, tally, maxima, rain
+        wall = float(sum(walls))
+        plain = {"wall_s": wall, "runs_per_h": 3600.0 * len(specs) / wall,
+                 "cell_steps_per_s": float(np.dot(cells, steps)) / wall, "steps": steps, "peak_depth": peak}  # fmt: skip
+    b0 = time.perf_counter()
+    B = Batch([i[0] for i in inputs], [i[1] for i in inputs], num)
+    B.set_boundary([i[2] for i in inputs])
+    B.set_depth([np.zeros(i[0].shape) for i in inputs])
+    B.set_tally([i[4] for i in inputs])
+    B.reset_envelope()
+    rc = [B.native_of(r, i[3]) for r, i in enumerate(inputs)]
+    torch.cuda.synchronize(dev)
+    pack_s = time.perf_counter() - b0
+    w0 = time.perf_counter()
+    books = B.run_windows(t_end, storms, window=30.0, max_every=4, cells=rc)
+    torch.cuda.synchronize(dev)
+    wall = time.perf_counter() - w0
+    bsteps = [int(x) for x in B.nsteps]
+    bpeak = [float(B.envelope(r)["depth"].max()) for r in range(len(specs))]
+    batch = {"wall_s": wall, "pack_s": pack_s, "runs_per_h": 3600.0 * len(specs) / wall,
+             "cell_steps_per_s": float(np.dot(cells, bsteps)) / wall, "loop_steps": int(max(bsteps)),
+             "tiles": int(B.grid.ntiles - 1)}  # fmt: skip
+    line = {
+        "run": "configuration 4 ensemble", "runs": len(specs), "cells": int(cells.sum()),
+        "sides": [sp.side for sp in specs], "simulated_h": [float(t) / 3600.0 for t in t_end],
+        "setup_s": setup, "batch": batch, "plain": plain,
+        "same_steps": None if plain is None else plain["steps"] == bsteps,
+        "same_peak_depth": None if plain is None else plain["peak_depth"] == bpeak,
+        "speedup": None if plain is None else plain["wall_s"] / wall,
+        "rain_m3": float(sum(b.rain for b in books)), "outflow_m3": float(sum(b.outflow for b in books)),
+    }  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     args = parse()
     if args.impl == "reference":
@@ -272,6 +381,9 @@ def main() -> None:
         return
     if args.full_run:
         full_run(args)
+        return
+    if args.ensemble:
+        ensemble_run(args)
         return
     import torch
     import torch.distributed as dist

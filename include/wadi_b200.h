@@ -46,9 +46,11 @@ enum W2BField {
     W2B_NFIELDS
 };
 
-/* Grid of wadi2d/grid/tiles.py:19-64: ny, nx padded to multiples of 32; ntiles includes the void tile 0. */
+/* Grid of wadi2d/grid/tiles.py:19-64: ny, nx padded to multiples of 32; ntiles includes the void tile 0. nruns > 1:
+ * a batch of independent runs packed into one grid, each run's padded grid on its own tiles (W2BBuffers.tile_run);
+ * a single run is nruns = 1. */
 typedef struct {
-    int32_t ny, nx, ntiles, rows;
+    int32_t ny, nx, ntiles, rows, nruns;
 } W2BGridDesc;
 
 /* The native layout of a grid, from w2b_layout. */
@@ -96,6 +98,9 @@ typedef struct {
     float *env[5];
     /* control block, W2B_CTL_BYTES bytes, 256-byte aligned */
     void *ctl;
+    /* the run table (w2b_run_table_bytes(nruns) bytes, 256-byte aligned) and the run of each tile (ntiles int32) */
+    void *runs;
+    const int32_t *tile_run;
     /* staging for REF_TILE transfers: ntiles * 1296 floats */
     float *stage;
 } W2BBuffers;
@@ -121,6 +126,9 @@ typedef struct {
 } W2BClock;
 
 int32_t w2b_version(void);
+
+/* Bytes of the run table of a batch of nruns runs. */
+int64_t w2b_run_table_bytes(int32_t nruns);
 
 /* Self-check of the step's float cube root (no counterpart in the reference): compares it, over count positive
  * floats from the bit pattern first_bits on, with the cube root rounded through double, as the reference's float32
@@ -213,12 +221,19 @@ typedef struct {
 int32_t w2b_cell_size(void* handle, float* dx);
 
 /* Replaces Forcing.rate's rain part (wadi2d/forcing.py:667-683) for a window [t0, t1]: writes src at the rained cells
- * and volume[0] (device) = the window's rain volume, m3 (float32 rates summed in FP64, times dx^2 (t1 - t0)). */
+ * and volume[0] (device) = the window's rain volume, m3 (float32 rates times the cell area of each cell's run, summed
+ * in FP64, times t1 - t0). */
 int32_t w2b_rain_window(void* handle, const W2BRain* rain, double f0, double f1, double t0, double t1,
                         double* volume, void* stream);
 
-/* Replaces Monitor.storage (wadi2d/engine/monitor.py:214-218): out[0] (device) = dx^2 * sum of h + res over the n
- * NATIVE cells, FP64. partial: W2B_PARTIALS doubles of scratch. */
+/* Uniform sources of a batch: src at each of the n NATIVE cells = rate[run of the cell] (device array of nruns,
+ * m/s). The batched form of Forcing.rate's uniform rain (wadi2d/storm/uniform.py:31-35, wadi2d/forcing.py:667-683)
+ * for runs that each have a storm of their own. */
+int32_t w2b_source_runs(void* handle, int64_t n, const int32_t* cells, const float* rate, void* stream);
+
+/* Replaces Monitor.storage (wadi2d/engine/monitor.py:214-218): out[0] (device) = sum of (h + res) dx^2 over the n
+ * NATIVE cells, FP64, each cell read from its run's current half with its run's cell size. partial: W2B_PARTIALS
+ * doubles of scratch. */
 int32_t w2b_storage(void* handle, int64_t n, const int32_t* cells, double* partial, double* out, void* stream);
 
 /* Inputs of the table builder (wadi2d/tables/builder.py:131-258; kernels of wadi2d/tables/core.py). Device pointers.
@@ -272,6 +287,20 @@ int32_t w2b_build_tables(const W2BTableIn* in, const W2BTableOut* out, void* str
  *    before reading it, so nothing has to start at zero. Calls that overlap on the GPU (two streams, two threads)
  *    race on it: serialise them. */
 int32_t w2b_build_tables_noalloc(const W2BTableIn* in, const W2BTableOut* out, void* stream);
+
+/* Batches (W2BGridDesc.nruns > 1): each run's cell size (host array of nruns), before its first advance. */
+int32_t w2b_set_run_dx(void* handle, const float* dx, int32_t n);
+
+/* Each run's current half of the ping-pong pairs (h, u, v, mx, my): out[r] in {0, 1}, host array of nruns. In a
+ * batch the runs' halves differ once their step counts do; w2b_field_ptr, w2b_get_field and w2b_set_field address
+ * run 0's half. */
+int32_t w2b_run_halves(void* handle, int32_t* out, void* stream);
+
+/* The device loop over a batch: every unfinished run advances by one of its own steps per loop step, until each
+ * reaches its t_end[r] (host array) or runs max_steps steps; clocks[r] in and out (host). Returns the first failing
+ * status, with each run's own in clocks[r].status. */
+int32_t w2b_advance_runs(void* handle, const W2BStepper* cfg, const double* t_end, int64_t max_steps,
+                         W2BClock* clocks, void* stream);
 
 #ifdef __cplusplus
 }

@@ -28,7 +28,7 @@ class W2BError(RuntimeError):
 
 
 class GridDesc(ctypes.Structure):
-    _fields_ = [("ny", c_i32), ("nx", c_i32), ("ntiles", c_i32), ("rows", c_i32)]
+    _fields_ = [("ny", c_i32), ("nx", c_i32), ("ntiles", c_i32), ("rows", c_i32), ("nruns", c_i32)]
 
 
 class Layout(ctypes.Structure):
@@ -49,7 +49,7 @@ class Buffers(ctypes.Structure):
         + [("dtab2", c_vp), ("ftab4", c_vp * 2)]
         + [(n, c_vp) for n in ("tiles", "tile_of", "nbr", "active", "wave", "wet", "keep", "idle", "is_act", "woken",
                                "scratch", "bmark")]  # fmt: skip
-        + [("env", c_vp * 5), ("ctl", c_vp), ("stage", c_vp)]
+        + [("env", c_vp * 5), ("ctl", c_vp), ("runs", c_vp), ("tile_run", c_vp), ("stage", c_vp)]
     )
 
 
@@ -96,6 +96,11 @@ _SIGNATURES = {
     "w2b_tally": [c_vp, c_f64, c_vp],
     "w2b_advance": [c_vp, ctypes.POINTER(Stepper), c_f64, c_i64, ctypes.POINTER(Clock), c_vp],
     "w2b_build_tables": [c_vp, c_vp, c_vp],
+    "w2b_run_table_bytes": [c_i32],
+    "w2b_set_run_dx": [c_vp, c_vp, c_i32],
+    "w2b_run_halves": [c_vp, c_vp, c_vp],
+    "w2b_source_runs": [c_vp, c_i64, c_vp, c_vp, c_vp],
+    "w2b_advance_runs": [c_vp, ctypes.POINTER(Stepper), c_vp, c_i64, c_vp, c_vp],
     "w2b_cell_size": [c_vp, ctypes.POINTER(c_f32)],
     "w2b_rain_window": [c_vp, c_vp, c_f64, c_f64, c_f64, c_f64, c_vp, c_vp],
     "w2b_storage": [c_vp, c_i64, c_vp, c_vp, c_vp, c_vp],
@@ -117,7 +122,7 @@ def lib() -> ctypes.CDLL:
         for name, args in _SIGNATURES.items():
             fn = getattr(L, name)
             fn.argtypes = args
-            fn.restype = c_i32
+            fn.restype = c_i64 if name == "w2b_run_table_bytes" else c_i32
         _lib = L
     return _lib
 

@@ -132,7 +132,7 @@ class B200Backend:
 
     name = "b200"
 
-    def __init__(self, tables: GridTables, num: NumericsRecord, device=None) -> None:
+    def __init__(self, tables: GridTables, num: NumericsRecord, device=None, tile_run=None, nruns: int = 1) -> None:
         import torch
 
         self.torch = torch
@@ -146,7 +146,8 @@ class B200Backend:
         ny, nx = g.shape
         nt = g.ntiles
         rows = self.rows
-        self._desc = _lib.GridDesc(ny, nx, nt, rows)
+        self.nruns = int(nruns)
+        self._desc = _lib.GridDesc(ny, nx, nt, rows, self.nruns)
         lay = _lib.Layout()
         _lib.call("w2b_layout", ctypes.byref(self._desc), ctypes.byref(lay))
         self.px, self.ncells = int(lay.px), int(lay.ncells)
@@ -191,6 +192,10 @@ class B200Backend:
         t["bmark"] = i32(nt * TILE)
         t["env"] = [f32(nt * TILE2, -1.0 if n == "arrival" else 0.0) for n in ENVELOPE]
         t["ctl"] = torch.zeros(_lib.CTL_BYTES // 8, dtype=torch.int64, device=dev)
+        nbytes = int(_lib.lib().w2b_run_table_bytes(self.nruns))
+        t["runs"] = torch.zeros((nbytes + 7) // 8, dtype=torch.int64, device=dev)
+        t["tile_run"] = (torch.zeros(nt, dtype=torch.int32, device=dev) if tile_run is None
+                         else torch.as_tensor(np.ascontiguousarray(tile_run, np.int32), device=dev))  # fmt: skip
         t["stage"] = f32(nt * STRIDE2)
         self._t = t
         # own cells of every allocated tile, NATIVE index in tile-layout order (fid = t * 1024 + j * 32 + i)
@@ -213,7 +218,7 @@ class B200Backend:
             getattr(B, n)[1] = t[n][1].data_ptr()
         for n in ("d", "qx", "qy", "qx1", "qy1", "res", "src", "om", "zcx", "zcy", "hc", "dtab2", "tiles", "tile_of",
                   "nbr", "active", "wave", "wet", "keep", "idle", "is_act", "woken", "scratch", "bmark", "ctl",
-                  "stage"):  # fmt: skip
+                  "runs", "tile_run", "stage"):  # fmt: skip
             setattr(B, n, t[n].data_ptr())
         for a, ax in enumerate("xy"):
             for f in ("fl", "fr", "gl", "gr", "ef", "cw"):

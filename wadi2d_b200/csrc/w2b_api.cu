@@ -6,6 +6,7 @@
 #include <cstdio>
 #include <cstring>
 #include <new>
+#include <vector>
 
 #include <cuda.h>
 
@@ -15,15 +16,16 @@ namespace w2b {
 cudaError_t faces_setup();
 void launch_cbrt_check(uint32_t first, uint32_t count, unsigned long long* out, cudaStream_t s);
 int faces_occupancy();
-void launch_faces(const TMaps& M, const StepArgs& A, int p, int grid, cudaStream_t s);
+void launch_faces(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s);
 cudaError_t update_setup();
 int update_occupancy();
-void launch_update(const TMaps& M, const StepArgs& A, int p, int grid, cudaStream_t s);
+void launch_update(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s);
 __global__ void boundary_kernel(StepArgs A, int control);
-__global__ void prestep_kernel(Ctl* ctl);
-__global__ void setstep_kernel(Ctl* ctl, float dtf, int want_wave, int want_wet, int nact);
+__global__ void prestep_kernel(StepArgs A);
+__global__ void setstep_kernel(StepArgs A, float dtf, int want_wave, int want_wet, int nact);
+__global__ void endstep_kernel(StepArgs A);
 __global__ void activity_kernel(StepArgs A);
-__global__ void plan_kernel(StepArgs A, const int32_t* list, int count, const float* h);
+__global__ void plan_kernel(StepArgs A, const int32_t* list, int count);
 __global__ void maxima_kernel(StepArgs A, float time, float arrive, float deep, int nact);
 __global__ void tally_kernel(StepArgs A, double dt);
 __global__ void ref_to_native_kernel(const float* ref, float* nat, const int32_t* tiles, int ntiles, int px);
@@ -34,8 +36,7 @@ __global__ void pack_tables_kernel(const float* dtab, const float* ftabx, const 
 __global__ void bmark_kernel(StepArgs A, int clear_words);
 
 struct Loop {
-    cudaGraphExec_t exec[2] = {nullptr, nullptr};  // by starting parity
-    int steps = 0;
+    cudaGraphExec_t exec = nullptr;
     unsigned version = ~0u;
 };
 
@@ -44,8 +45,10 @@ struct Handle {
     W2BLayout L{};
     W2BParams P{};
     W2BBuffers B{};
-    int cur = 0;
+    int cur = 0;  // run 0's current half (the device keeps it in R.parity[0])
     int nact = 0;
+    int nruns = 1;
+    RunTab R;
     int nb = 0;
     const int32_t *bcell = nullptr, *bref = nullptr, *bkind = nullptr;
     const float *bd0 = nullptr, *bh0 = nullptr;
@@ -63,27 +66,22 @@ struct Handle {
     Ctl* ctl() const { return reinterpret_cast<Ctl*>(B.ctl); }
 };
 
-static StepArgs make_args(const Handle& H, int p) {
+static StepArgs make_args(const Handle& H) {
     StepArgs A;
     memset(&A, 0, sizeof(A));
-    const int n = 1 - p;
     A.P = H.P;
     A.rows = H.g.rows;
     A.px = H.L.px;
     A.ntiles = H.g.ntiles;
     A.nty = H.g.ny / TILE;
     A.ntx = H.g.nx / TILE;
-    A.area = H.P.dx * H.P.dx;
-    A.h = H.B.h[p];
-    A.h_next = H.B.h[n];
-    A.u[0] = H.B.u[p];
-    A.u[1] = H.B.v[p];
-    A.u_next[0] = H.B.u[n];
-    A.u_next[1] = H.B.v[n];
-    A.m[0] = H.B.mx[p];
-    A.m[1] = H.B.my[p];
-    A.m_next[0] = H.B.mx[n];
-    A.m_next[1] = H.B.my[n];
+    for (int q = 0; q < 2; ++q) {
+        A.hh[q] = H.B.h[q];
+        A.uu[0][q] = H.B.u[q];
+        A.uu[1][q] = H.B.v[q];
+        A.mm[0][q] = H.B.mx[q];
+        A.mm[1][q] = H.B.my[q];
+    }
     A.d = H.B.d;
     A.q[0] = H.B.qx;
     A.q[1] = H.B.qy;
@@ -130,7 +128,16 @@ static StepArgs make_args(const Handle& H, int p) {
     A.tsign = H.tsign;
     A.ttotal = H.ttotal;
     A.ctl = H.ctl();
+    A.tile_run = H.B.tile_run;
+    A.R = H.R;
+    A.nruns = H.nruns;
     return A;
+}
+
+bool handle_args(void* handle, StepArgs* out) {
+    if (!handle || !out) return false;
+    *out = make_args(*static_cast<Handle*>(handle));
+    return true;
 }
 
 static int cuda_status(cudaError_t e, const char* where) {
@@ -207,25 +214,24 @@ static int build_tmaps(Handle& H) {
 }
 
 static void drop_graphs(Handle& H) {
-    for (auto& e : H.loop.exec)
-        if (e) {
-            cudaGraphExecDestroy(e);
-            e = nullptr;
-        }
+    if (H.loop.exec) {
+        cudaGraphExecDestroy(H.loop.exec);
+        H.loop.exec = nullptr;
+    }
     H.loop.version = ~0u;
 }
 
-// One step of the device loop, parity p.
-static int launch_loop_step(Handle& H, int p, cudaStream_t s) {
-    const StepArgs A = make_args(H, p);
+// One step of the device loop: every running run advances by one of its own steps.
+static int launch_loop_step(Handle& H, cudaStream_t s) {
+    const StepArgs A = make_args(H);
     const dim3 blk(32, 8);
     const int grid = blocks_for(H, H.g.ntiles - 1);
-    prestep_kernel<<<1, 1, 0, s>>>(A.ctl);
-    launch_faces(H.tmaps, A, p, faces_grid(H, H.g.ntiles - 1), s);
-    launch_update(H.tmaps, A, p, grid, s);
+    prestep_kernel<<<1, 1024, 0, s>>>(A);
+    launch_faces(H.tmaps, A, faces_grid(H, H.g.ntiles - 1), s);
+    launch_update(H.tmaps, A, grid, s);
     boundary_kernel<<<1, 256, 0, s>>>(A, 1);
     activity_kernel<<<1, 1024, 0, s>>>(A);
-    plan_kernel<<<grid, blk, 0, s>>>(A, A.woken, -1, A.h_next);
+    plan_kernel<<<grid, blk, 0, s>>>(A, A.woken, -1);
     CKL("loop step");
     return W2B_OK;
 }
@@ -236,7 +242,9 @@ using namespace w2b;
 
 extern "C" {
 
-int32_t w2b_version(void) { return 1; }
+int32_t w2b_version(void) { return 2; }
+
+int64_t w2b_run_table_bytes(int32_t nruns) { return nruns < 1 ? 0 : (int64_t)run_table_bytes(nruns); }
 
 int32_t w2b_selftest_cbrt(uint32_t first_bits, uint32_t count, uint64_t* out, void* stream) {
     if (!out) return W2B_EINVAL;
@@ -274,7 +282,8 @@ int32_t w2b_ref_to_native(const W2BGridDesc* grid, const int32_t* tiles_host, in
 
 int32_t w2b_create(const W2BGridDesc* grid, const W2BParams* params, const W2BBuffers* buffers, void** handle) {
     if (!grid || !params || !buffers || !handle) return W2B_EINVAL;
-    if (grid->rows < 4 || grid->rows > 64) return W2B_EINVAL;
+    if (grid->rows < 4 || grid->rows > 64 || grid->nruns < 1) return W2B_EINVAL;
+    if (!buffers->runs || ((uintptr_t)buffers->runs & 255) || !buffers->tile_run) return W2B_EINVAL;
     Handle* H = new (std::nothrow) Handle();
     if (!H) return W2B_EINVAL;
     H->g = *grid;
@@ -304,6 +313,12 @@ int32_t w2b_create(const W2BGridDesc* grid, const W2BParams* params, const W2BBu
         return W2B_ECUDA;
     }
     H->nact = grid->ntiles - 1;
+    H->nruns = grid->nruns;
+    H->R = run_table(H->B.runs, H->nruns);
+    if (H->nruns == 1 && cudaMemcpy(H->R.dx, &H->P.dx, sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+        delete H;
+        return cuda_status(cudaGetLastError(), "w2b_create run table");
+    }
     if (cudaStreamCreateWithFlags(&H->cap, cudaStreamNonBlocking) != cudaSuccess) {
         delete H;
         return cuda_status(cudaGetLastError(), "w2b_create stream");
@@ -338,6 +353,7 @@ int32_t w2b_set_params(void* handle, const W2BParams* params) {
     Handle* H = static_cast<Handle*>(handle);
     H->P = *params;
     H->version++;
+    if (H->nruns == 1) CK(cudaMemcpy(H->R.dx, &H->P.dx, sizeof(float), cudaMemcpyHostToDevice));
     return W2B_OK;
 }
 
@@ -363,7 +379,7 @@ int32_t w2b_set_boundary(void* handle, int32_t n, const int32_t* cell, const int
     H->bd0 = d0;
     H->bh0 = h0;
     H->version++;
-    const StepArgs A = make_args(*H, H->cur);
+    const StepArgs A = make_args(*H);
     bmark_kernel<<<64, 256>>>(A, H->g.ntiles * TILE);
     if (n) bmark_kernel<<<64, 256>>>(A, 0);
     CKL("w2b_set_boundary");
@@ -387,17 +403,19 @@ int32_t w2b_step(void* handle, float dt, int32_t want_wave, int32_t want_wet, vo
     if (!handle) return W2B_EINVAL;
     Handle* H = static_cast<Handle*>(handle);
     cudaStream_t s = (cudaStream_t)stream;
+    if (H->nruns != 1) return W2B_EINVAL;  // a batch steps in the device loop
     if (want_wave) CK(cudaMemsetAsync(H->B.wave, 0, sizeof(float) * H->g.ntiles, s));
-    setstep_kernel<<<1, 1, 0, s>>>(H->ctl(), dt, want_wave, want_wet, H->nact);
-    if (H->nact == 0) {
+    const StepArgs A = make_args(*H);
+    setstep_kernel<<<1, 1, 0, s>>>(A, dt, want_wave, want_wet, H->nact);
+    if (H->nact == 0) {  // as the reference: no tiles, no swap
         CKL("w2b_step");
         return W2B_OK;
     }
-    const StepArgs A = make_args(*H, H->cur);
     const int grid = blocks_for(*H, H->nact);
-    launch_faces(H->tmaps, A, H->cur, faces_grid(*H, H->nact), s);
-    launch_update(H->tmaps, A, H->cur, grid, s);
+    launch_faces(H->tmaps, A, faces_grid(*H, H->nact), s);
+    launch_update(H->tmaps, A, grid, s);
     if (H->nb) boundary_kernel<<<1, 256, 0, s>>>(A, 0);
+    endstep_kernel<<<1, 1, 0, s>>>(A);
     CKL("w2b_step");
     H->cur ^= 1;
     return W2B_OK;
@@ -407,19 +425,20 @@ int32_t w2b_step_timed(void* handle, float dt, int32_t want_wave, int32_t want_w
     if (!handle || !ms) return W2B_EINVAL;
     Handle* H = static_cast<Handle*>(handle);
     cudaStream_t s = (cudaStream_t)stream;
-    if (H->nact == 0) return W2B_EINVAL;
+    if (H->nact == 0 || H->nruns != 1) return W2B_EINVAL;
     cudaEvent_t ev[4];
     for (auto& e : ev) CK(cudaEventCreate(&e));
     if (want_wave) CK(cudaMemsetAsync(H->B.wave, 0, sizeof(float) * H->g.ntiles, s));
-    setstep_kernel<<<1, 1, 0, s>>>(H->ctl(), dt, want_wave, want_wet, H->nact);
-    const StepArgs A = make_args(*H, H->cur);
+    const StepArgs A = make_args(*H);
+    setstep_kernel<<<1, 1, 0, s>>>(A, dt, want_wave, want_wet, H->nact);
     const int grid = blocks_for(*H, H->nact);
     CK(cudaEventRecord(ev[0], s));
-    launch_faces(H->tmaps, A, H->cur, faces_grid(*H, H->nact), s);
+    launch_faces(H->tmaps, A, faces_grid(*H, H->nact), s);
     CK(cudaEventRecord(ev[1], s));
-    launch_update(H->tmaps, A, H->cur, grid, s);
+    launch_update(H->tmaps, A, grid, s);
     CK(cudaEventRecord(ev[2], s));
     if (H->nb) boundary_kernel<<<1, 256, 0, s>>>(A, 0);
+    endstep_kernel<<<1, 1, 0, s>>>(A);
     CK(cudaEventRecord(ev[3], s));
     CKL("w2b_step_timed");
     H->cur ^= 1;
@@ -433,7 +452,7 @@ int32_t w2b_max_wave(void* handle, float* out, void* stream) {
     if (!handle || !out) return W2B_EINVAL;
     Handle* H = static_cast<Handle*>(handle);
     int32_t status = 0;
-    CK(cudaMemcpyAsync(out, &H->ctl()->wave_max, sizeof(float), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
+    CK(cudaMemcpyAsync(out, H->R.wave_bits, sizeof(float), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
     CK(cudaMemcpyAsync(&status, &H->ctl()->status, sizeof(int32_t), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
     CK(cudaStreamSynchronize((cudaStream_t)stream));
     return status == W2B_ETIMEOUT ? W2B_ETIMEOUT : W2B_OK;
@@ -451,8 +470,8 @@ int32_t w2b_refresh_plan(void* handle, const int32_t* tiles, int32_t n, void* st
     if (!handle || n < 0 || (n && !tiles)) return W2B_EINVAL;
     Handle* H = static_cast<Handle*>(handle);
     if (!n) return W2B_OK;
-    const StepArgs A = make_args(*H, H->cur);
-    plan_kernel<<<blocks_for(*H, n), dim3(32, 8), 0, (cudaStream_t)stream>>>(A, tiles, n, H->B.h[H->cur]);
+    const StepArgs A = make_args(*H);
+    plan_kernel<<<blocks_for(*H, n), dim3(32, 8), 0, (cudaStream_t)stream>>>(A, tiles, n);
     CKL("w2b_refresh_plan");
     return W2B_OK;
 }
@@ -550,9 +569,7 @@ int32_t w2b_maxima(void* handle, float t, float arrive, float deep, void* stream
     if (!handle) return W2B_EINVAL;
     Handle* H = static_cast<Handle*>(handle);
     if (!H->nact) return W2B_OK;
-    StepArgs A = make_args(*H, H->cur);
-    A.u_next[0] = H->B.u[H->cur];  // the envelope reads the state after the step
-    A.u_next[1] = H->B.v[H->cur];
+    const StepArgs A = make_args(*H);
     maxima_kernel<<<blocks_for(*H, H->nact), dim3(32, 8), 0, (cudaStream_t)stream>>>(A, t, arrive, deep, H->nact);
     CKL("w2b_maxima");
     return W2B_OK;
@@ -562,86 +579,140 @@ int32_t w2b_tally(void* handle, double dt, void* stream) {
     if (!handle) return W2B_EINVAL;
     Handle* H = static_cast<Handle*>(handle);
     if (!H->ntally) return W2B_OK;
-    const StepArgs A = make_args(*H, H->cur);
+    const StepArgs A = make_args(*H);
     tally_kernel<<<(H->ntally + 255) / 256, 256, 0, (cudaStream_t)stream>>>(A, dt);
     CKL("w2b_tally");
     return W2B_OK;
 }
 
-// The device-resident loop. Steps run in chunks of a captured graph of LOOP_STEPS steps (an even number, so a chunk
-// that runs to its end leaves the parity where it found it); after each chunk the host reads the clock once.
+// The device-resident loop. Steps run in chunks of a captured graph of LOOP_STEPS steps, every running run advancing
+// one of its own steps each graph step; after each chunk the host reads the runs' clocks once.
 static constexpr int LOOP_STEPS = 16;
+
+static int advance_runs(Handle* H, const W2BStepper* cfg, const double* t_end, int64_t max_steps, W2BClock* clocks,
+                        cudaStream_t s) {
+    const int n = H->nruns;
+    Ctl c;
+    memset(&c, 0, sizeof(c));
+    c.nact = H->nact;
+    c.nruns = n;
+    c.dt_every = cfg->dt_every;
+    c.active_every = cfg->active_every;
+    c.adaptive = cfg->adaptive;
+    c.max_every = cfg->max_every;
+    c.arrive = cfg->arrive;
+    c.deep = cfg->deep;
+    c.cfl = cfg->cfl;
+    c.wave_floor = cfg->wave_floor;
+    c.dt_max = cfg->dt_max;
+    c.dt_min = cfg->dt_min;
+    std::vector<double> t(n), dt(n), te(t_end, t_end + n);
+    std::vector<long long> ns(n), zero(n, 0), ms(n, (long long)max_steps);
+    std::vector<int32_t> rd(n), st(n, 0);
+    for (int r = 0; r < n; ++r) {
+        t[r] = clocks[r].t;
+        dt[r] = clocks[r].dt;
+        ns[r] = clocks[r].nsteps;
+        rd[r] = clocks[r].refresh_due;
+    }
+    const RunTab& R = H->R;
+    CK(cudaMemcpyAsync(H->ctl(), &c, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(R.t, t.data(), 8 * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(R.dt, dt.data(), 8 * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(R.t_end, te.data(), 8 * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(R.nsteps, ns.data(), 8 * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(R.steps_run, zero.data(), 8 * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(R.max_steps, ms.data(), 8 * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(R.refresh_due, rd.data(), 4 * n, cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(R.status, st.data(), 4 * n, cudaMemcpyHostToDevice, s));
+    if (H->loop.version != H->version) {
+        drop_graphs(*H);
+        cudaGraph_t graph;
+        CK(cudaStreamBeginCapture(H->cap, cudaStreamCaptureModeThreadLocal));
+        int stc = W2B_OK;
+        for (int k = 0; k < LOOP_STEPS && stc == W2B_OK; ++k) stc = launch_loop_step(*H, H->cap);
+        cudaError_t e = cudaStreamEndCapture(H->cap, &graph);
+        if (stc != W2B_OK) return stc;
+        CK(e);
+        e = cudaGraphInstantiate(&H->loop.exec, graph, 0);
+        cudaGraphDestroy(graph);
+        CK(e);
+        H->loop.version = H->version;
+    }
+    std::vector<long long> run(n);
+    int32_t gstatus = 0;
+    for (;;) {
+        CK(cudaGraphLaunch(H->loop.exec, s));
+        CK(cudaMemcpyAsync(t.data(), R.t, 8 * n, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(run.data(), R.steps_run, 8 * n, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(st.data(), R.status, 4 * n, cudaMemcpyDeviceToHost, s));
+        CK(cudaMemcpyAsync(&gstatus, &H->ctl()->status, 4, cudaMemcpyDeviceToHost, s));
+        CK(cudaStreamSynchronize(s));
+        bool done = gstatus != 0;
+        if (!done) {
+            done = true;
+            for (int r = 0; r < n; ++r)
+                if (st[r] == 0 && t[r] < te[r] - 1e-9 && run[r] < ms[r]) done = false;
+        }
+        if (done) break;
+    }
+    std::vector<uint32_t> wb(n);
+    std::vector<int32_t> par(n);
+    CK(cudaMemcpyAsync(dt.data(), R.dt, 8 * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(ns.data(), R.nsteps, 8 * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(wb.data(), R.wave_bits, 4 * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(par.data(), R.parity, 4 * n, cudaMemcpyDeviceToHost, s));
+    int32_t nact = 0;
+    CK(cudaMemcpyAsync(&nact, &H->ctl()->nact, 4, cudaMemcpyDeviceToHost, s));
+    CK(cudaStreamSynchronize(s));
+    H->nact = nact;
+    H->cur = par[0];
+    int32_t first = gstatus;
+    for (int r = 0; r < n; ++r) {
+        clocks[r].t = t[r];
+        clocks[r].dt = dt[r];
+        clocks[r].nsteps = ns[r];
+        clocks[r].refresh_due = 0;
+        clocks[r].status = st[r] != 0 ? st[r] : gstatus;
+        float w;
+        memcpy(&w, &wb[r], 4);
+        clocks[r].wave_max = w;
+        clocks[r].nact = nact;
+        if (!first && st[r]) first = st[r];
+    }
+    return first;
+}
 
 int32_t w2b_advance(void* handle, const W2BStepper* cfg, double t_end, int64_t max_steps, W2BClock* clock,
                     void* stream) {
     if (!handle || !cfg || !clock || max_steps < 0 || cfg->dt_every < 1 || cfg->active_every < 1) return W2B_EINVAL;
     Handle* H = static_cast<Handle*>(handle);
+    if (H->nruns != 1) return W2B_EINVAL;
+    return advance_runs(H, cfg, &t_end, max_steps, clock, (cudaStream_t)stream);
+}
+
+int32_t w2b_advance_runs(void* handle, const W2BStepper* cfg, const double* t_end, int64_t max_steps,
+                         W2BClock* clocks, void* stream) {
+    if (!handle || !cfg || !clocks || !t_end || max_steps < 0 || cfg->dt_every < 1 || cfg->active_every < 1)
+        return W2B_EINVAL;
+    return advance_runs(static_cast<Handle*>(handle), cfg, t_end, max_steps, clocks, (cudaStream_t)stream);
+}
+
+int32_t w2b_run_halves(void* handle, int32_t* out, void* stream) {
+    if (!handle || !out) return W2B_EINVAL;
+    Handle* H = static_cast<Handle*>(handle);
     cudaStream_t s = (cudaStream_t)stream;
-    // clock and settings into the control block
-    Ctl init;
-    CK(cudaMemcpyAsync(&init, H->ctl(), sizeof(Ctl), cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(out, H->R.parity, sizeof(int32_t) * H->nruns, cudaMemcpyDeviceToHost, s));
     CK(cudaStreamSynchronize(s));
-    init.t = clock->t;
-    init.dt = clock->dt;
-    init.t_end = t_end;
-    init.nsteps = clock->nsteps;
-    init.steps_run = 0;
-    init.max_steps = max_steps;
-    init.refresh_due = clock->refresh_due;
-    init.status = 0;
-    init.nact = H->nact;
-    init.ticket = 0u;
-    init.run = 1;
-    init.cfl = cfg->cfl;
-    init.wave_floor = cfg->wave_floor;
-    init.dt_max = cfg->dt_max;
-    init.dt_min = cfg->dt_min;
-    init.dx = (double)H->P.dx;
-    init.dt_every = cfg->dt_every;
-    init.active_every = cfg->active_every;
-    init.adaptive = cfg->adaptive;
-    init.max_every = cfg->max_every;
-    init.arrive = cfg->arrive;
-    init.deep = cfg->deep;
-    init.want_max = 0;
-    CK(cudaMemcpyAsync(H->ctl(), &init, sizeof(Ctl), cudaMemcpyHostToDevice, s));
-    // graphs for both starting parities, rebuilt when an argument they captured has changed
-    if (H->loop.version != H->version) {
-        drop_graphs(*H);
-        for (int p0 = 0; p0 < 2; ++p0) {
-            cudaGraph_t graph;
-            CK(cudaStreamBeginCapture(H->cap, cudaStreamCaptureModeThreadLocal));
-            int st = W2B_OK;
-            for (int k = 0; k < LOOP_STEPS && st == W2B_OK; ++k) st = launch_loop_step(*H, (p0 + k) & 1, H->cap);
-            cudaError_t e = cudaStreamEndCapture(H->cap, &graph);
-            if (st != W2B_OK) return st;
-            CK(e);
-            e = cudaGraphInstantiate(&H->loop.exec[p0], graph, 0);
-            cudaGraphDestroy(graph);
-            CK(e);
-        }
-        H->loop.version = H->version;
-    }
-    Ctl now;
-    long long done = 0;
-    for (;;) {
-        CK(cudaGraphLaunch(H->loop.exec[H->cur], s));
-        CK(cudaMemcpyAsync(&now, H->ctl(), sizeof(Ctl), cudaMemcpyDeviceToHost, s));
-        CK(cudaStreamSynchronize(s));
-        const long long ran = now.steps_run - done;
-        done = now.steps_run;
-        H->cur ^= (int)(ran & 1);
-        if (now.status != 0 || !(now.t < t_end - 1e-9) || now.steps_run >= max_steps || ran < LOOP_STEPS) break;
-    }
-    H->nact = now.nact;
-    clock->t = now.t;
-    clock->dt = now.dt;
-    clock->nsteps = now.nsteps;
-    clock->refresh_due = 0;
-    clock->status = now.status;
-    clock->wave_max = now.wave_max;
-    clock->nact = now.nact;
-    return now.status;
+    return W2B_OK;
+}
+
+int32_t w2b_set_run_dx(void* handle, const float* dx, int32_t n) {
+    if (!handle || !dx) return W2B_EINVAL;
+    Handle* H = static_cast<Handle*>(handle);
+    if (n != H->nruns) return W2B_EINVAL;
+    CK(cudaMemcpy(H->R.dx, dx, sizeof(float) * n, cudaMemcpyHostToDevice));
+    return W2B_OK;
 }
 
 }  // extern "C"

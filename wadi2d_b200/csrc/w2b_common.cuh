@@ -18,47 +18,72 @@ constexpr int GY = 4;   // guard rows above and below the padded grid in the nat
 constexpr int GX = 32;  // guard columns left and right: keeps every tile row 128-byte aligned
 constexpr int SLEEP_CHECKS = 2;  // wadi2d/solver/stepper.py:12
 
-// Device control block, W2B_CTL_BYTES long. Written by the host's set-step kernel or by the device loop's control
-// kernel, read by every step kernel.
+// Device control block, W2B_CTL_BYTES long: what the step kernels share across runs. Each run's own clock and step
+// settings live in the run table (RunTab); a single run is run 0 of a table of one.
 struct Ctl {
-    // this step
-    float dtf;          // dt as the kernels take it, float32
-    int32_t run;        // 0: the device loop has finished, kernels return at once
-    int32_t want_wave;  // refresh step: wave speeds and the wet share om
-    int32_t want_wet;   // active-list step: tile wet flags
-    int32_t want_max;   // envelope step
-    float max_time;     // envelope time (float32 of t after the step)
-    double dt_tally;    // t after the step minus t before it, FP64
-    double dt_step;     // this step's dt, FP64 (the device loop)
-    int32_t nact;       // active tiles
-    uint32_t ticket;    // last-block counter of the wave reduction
-    float wave_max;     // max wave over active tiles of the last refresh step
-    int32_t activate;   // this step rebuilds the active list (device loop)
-    // device loop clock (wadi2d/solver/stepper.py:24-47)
-    double t, dt, t_end;
-    long long nsteps, steps_run, max_steps;
-    int32_t refresh_due, status;
-    int32_t nwoken;
-    int32_t pad0;
-    // stepper settings
-    double cfl, wave_floor, dt_max, dt_min, dx;
+    int32_t nact;       // active tiles (all runs)
+    uint32_t any;       // ANY_* bits: OR over the runs of this step's flags
+    int32_t nwoken;     // tiles the last rebuild woke
+    int32_t status;     // a failure no single run owns (W2B_ETIMEOUT)
+    int32_t nruns;
     int32_t dt_every, active_every, adaptive, max_every;
     float arrive, deep;
+    double cfl, wave_floor, dt_max, dt_min;
 };
 static_assert(sizeof(Ctl) <= W2B_CTL_BYTES, "control block too large");
+
+constexpr uint32_t ANY_RUN = 1u, ANY_WAVE = 2u, ANY_ACT = 4u;
+// per-run flags of this step
+constexpr int32_t F_RUN = 1, F_WAVE = 2, F_WET = 4, F_MAX = 8, F_ACT = 16;
+
+// Per-run state, one entry a run (wadi2d/solver/stepper.py:24-47 for each run of a batch).
+struct RunTab {
+    double *t, *dt, *t_end, *dt_step, *dt_tally;
+    long long *nsteps, *steps_run, *max_steps;
+    float *dtf, *max_time, *dx;
+    int32_t *flags, *refresh_due, *status;
+    uint32_t* wave_bits;  // max wave speed of the run's tiles, as float bits (waves are never negative)
+    int32_t* parity;      // the run's current half of the ping-pong pairs
+};
+
+// Layout of a run table of nruns entries in one device block: each array 256-byte aligned.
+__host__ __device__ inline size_t run_table_bytes(int nruns) {
+    const size_t a = ((size_t)nruns * 8 + 255) / 256 * 256, b = ((size_t)nruns * 4 + 255) / 256 * 256;
+    return 8 * a + 8 * b;
+}
+
+__host__ __device__ inline RunTab run_table(void* base, int nruns) {
+    const size_t a = ((size_t)nruns * 8 + 255) / 256 * 256, b = ((size_t)nruns * 4 + 255) / 256 * 256;
+    char* p = static_cast<char*>(base);
+    RunTab R;
+    R.t = reinterpret_cast<double*>(p);
+    R.dt = reinterpret_cast<double*>(p + a);
+    R.t_end = reinterpret_cast<double*>(p + 2 * a);
+    R.dt_step = reinterpret_cast<double*>(p + 3 * a);
+    R.dt_tally = reinterpret_cast<double*>(p + 4 * a);
+    R.nsteps = reinterpret_cast<long long*>(p + 5 * a);
+    R.steps_run = reinterpret_cast<long long*>(p + 6 * a);
+    R.max_steps = reinterpret_cast<long long*>(p + 7 * a);
+    char* q = p + 8 * a;
+    R.dtf = reinterpret_cast<float*>(q);
+    R.max_time = reinterpret_cast<float*>(q + b);
+    R.dx = reinterpret_cast<float*>(q + 2 * b);
+    R.flags = reinterpret_cast<int32_t*>(q + 3 * b);
+    R.refresh_due = reinterpret_cast<int32_t*>(q + 4 * b);
+    R.status = reinterpret_cast<int32_t*>(q + 5 * b);
+    R.wave_bits = reinterpret_cast<uint32_t*>(q + 6 * b);
+    R.parity = reinterpret_cast<int32_t*>(q + 7 * b);
+    return R;
+}
 
 // Everything a step kernel reads, with the ping-pong halves resolved for one parity.
 struct StepArgs {
     W2BParams P;
     int32_t rows, px, ntiles, nty, ntx;
-    float area;  // dx * dx
-    // state, native
-    const float* __restrict__ h;  // current mean depth
-    float* __restrict__ h_next;
-    const float* __restrict__ u[2];  // current face velocities, x then y
-    float* __restrict__ u_next[2];
-    const float* __restrict__ m[2];  // current face momenta
-    float* __restrict__ m_next[2];
+    // state, native; ping-pong pairs by half: a run's current half is R.parity[run], the other is the next
+    float* hh[2];     // mean depth
+    float* uu[2][2];  // face velocities [axis x, y][half]
+    float* mm[2][2];  // face momenta [axis][half]
     float* __restrict__ d;
     float* __restrict__ q[2];   // qx, qy: scaled discharges
     float* __restrict__ q1[2];  // qx1, qy1: unscaled, from the face pass
@@ -102,6 +127,10 @@ struct StepArgs {
     const float* __restrict__ tsign;
     double* __restrict__ ttotal;
     Ctl* ctl;
+    // runs: the run of each tile, and the run table
+    const int32_t* __restrict__ tile_run;
+    RunTab R;
+    int32_t nruns;
 };
 
 // Tensor maps of the NATIVE state arrays for the face pass's TMA boxes: 40 x 36 floats (the tile, two cells of halo
@@ -227,5 +256,22 @@ __device__ __forceinline__ void face_lookup(float e, float top, const float4* __
     T = q.y + f * (q.w - q.y);
     W = (q.z - q.x) / de;
 }
+
+// The tile holding NATIVE index k, and the tile-layout index of k's cell.
+__device__ __forceinline__ int tile_of_native(const StepArgs& A, int k) {
+    const int j = k / A.px - GY;
+    const int i = k - (j + GY) * A.px - GX;
+    return A.tile_of[(j / TILE) * A.ntx + (i / TILE)];
+}
+
+__device__ __forceinline__ int fid_of_native(const StepArgs& A, int k) {
+    const int j = k / A.px - GY;
+    const int i = k - (j + GY) * A.px - GX;
+    const int t = A.tile_of[(j / TILE) * A.ntx + (i / TILE)];
+    return t * TILE2 + (j % TILE) * TILE + (i % TILE);
+}
+
+// The step arguments of a handle (for kernels of other translation units); false on a null handle.
+bool handle_args(void* handle, StepArgs* out);
 
 }  // namespace w2b

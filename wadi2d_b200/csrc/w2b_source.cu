@@ -4,8 +4,9 @@
 //
 // The rate restates wadi2d/forcing.py:667-683 per cell: excess = (E(P1) - E(P0)) / (1000 dt), with the SCS loss of
 // wadi2d/hydrology/losses.py:69-72 or the initial-and-constant loss of wadi2d_b200/forcing.py; the window's rain
-// volume is the sum of the float32 rates in FP64 times the cell area and dt. Storage restates
-// wadi2d/engine/monitor.py:214-218 (h + res over the interior cells, FP64).
+// volume is the sum of the float32 rates times the cell area in FP64, times dt. Storage restates
+// wadi2d/engine/monitor.py:214-218 (h + res over the interior cells, FP64). Each cell is weighed by the area of its
+// run's cells and its mean depth read from its run's current half, so one call serves a batch of runs as well.
 #include <cstdio>
 
 #include "w2b_common.cuh"
@@ -25,8 +26,14 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
     return red[0];
 }
 
-__global__ void __launch_bounds__(SRC_THREADS) rain_kernel(W2BRain R, float* __restrict__ src, double f0, double f1,
-                                                           double dt) {
+// The cell area of NATIVE index k's run.
+__device__ __forceinline__ double cell_area(const StepArgs& A, int k) {
+    const double dx = (double)A.R.dx[A.tile_run[tile_of_native(A, k)]];
+    return dx * dx;
+}
+
+__global__ void __launch_bounds__(SRC_THREADS) rain_kernel(StepArgs A, W2BRain R, double f0, double f1, double dt) {
+    float* src = const_cast<float*>(A.src);
     __shared__ double red[SRC_THREADS];
     double acc = 0.0;
     for (int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; m < R.n; m += (int64_t)gridDim.x * blockDim.x) {
@@ -54,25 +61,36 @@ __global__ void __launch_bounds__(SRC_THREADS) rain_kernel(W2BRain R, float* __r
             mm = p1 - p0;
         }
         const float rate = (float)(mm / (1000.0 * dt));
-        src[R.cells[m]] = rate;
-        acc += (double)rate;
+        const int k = R.cells[m];
+        src[k] = rate;
+        acc += (double)rate * cell_area(A, k);
     }
     const double b = block_sum(acc, red);
     if (threadIdx.x == 0) R.partial[blockIdx.x] = b;
 }
 
-__global__ void __launch_bounds__(SRC_THREADS) storage_kernel(int64_t n, const int32_t* __restrict__ cells,
-                                                              const float* __restrict__ h,
-                                                              const float* __restrict__ res,
+__global__ void __launch_bounds__(SRC_THREADS) storage_kernel(StepArgs A, int64_t n, const int32_t* __restrict__ cells,
                                                               double* __restrict__ partial) {
     __shared__ double red[SRC_THREADS];
     double acc = 0.0;
     for (int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; m < n; m += (int64_t)gridDim.x * blockDim.x) {
         const int k = cells[m];
-        acc += (double)h[k] + (double)res[k];
+        const float* h = A.hh[A.R.parity[A.tile_run[tile_of_native(A, k)]]];
+        acc += ((double)h[k] + (double)A.res[k]) * cell_area(A, k);
     }
     const double b = block_sum(acc, red);
     if (threadIdx.x == 0) partial[blockIdx.x] = b;
+}
+
+// src at each listed cell = its run's rate (a batch of runs under uniform rain of their own).
+__global__ void __launch_bounds__(SRC_THREADS) source_runs_kernel(StepArgs A, int64_t n,
+                                                                  const int32_t* __restrict__ cells,
+                                                                  const float* __restrict__ rate) {
+    float* src = const_cast<float*>(A.src);
+    for (int64_t m = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; m < n; m += (int64_t)gridDim.x * blockDim.x) {
+        const int k = cells[m];
+        src[k] = rate[A.tile_run[tile_of_native(A, k)]];
+    }
 }
 
 // out[0] = scale * (sum of the partials, in order)
@@ -96,14 +114,12 @@ int32_t w2b_rain_window(void* handle, const W2BRain* rain, double f0, double f1,
     if (!handle || !rain || !volume || !(t1 > t0) || rain->n < 0 || (rain->n && (!rain->cells || !rain->depth)) ||
         !rain->partial || (rain->loss == 1 && (!rain->s_mm || !rain->ia_mm)) || (rain->loss == 2 && !rain->ia_mm))
         return W2B_EINVAL;
-    float* src = nullptr;
-    if (w2b_field_ptr(handle, W2B_SRC, &src) != W2B_OK) return W2B_EINVAL;
-    float dx = 0.0f;
-    if (w2b_cell_size(handle, &dx) != W2B_OK) return W2B_EINVAL;
+    StepArgs A;
+    if (!handle_args(handle, &A)) return W2B_EINVAL;
     cudaStream_t s = (cudaStream_t)stream;
     const double dt = t1 - t0;
-    rain_kernel<<<SRC_BLOCKS, SRC_THREADS, 0, s>>>(*rain, src, f0, f1, dt);
-    finish_kernel<<<1, SRC_THREADS, 0, s>>>(rain->partial, SRC_BLOCKS, (double)dx * (double)dx * dt, volume);
+    rain_kernel<<<SRC_BLOCKS, SRC_THREADS, 0, s>>>(A, *rain, f0, f1, dt);
+    finish_kernel<<<1, SRC_THREADS, 0, s>>>(rain->partial, SRC_BLOCKS, dt, volume);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         fprintf(stderr, "libwadi_b200: w2b_rain_window: %s\n", cudaGetErrorString(e));
@@ -112,16 +128,26 @@ int32_t w2b_rain_window(void* handle, const W2BRain* rain, double f0, double f1,
     return W2B_OK;
 }
 
+int32_t w2b_source_runs(void* handle, int64_t n, const int32_t* cells, const float* rate, void* stream) {
+    if (!handle || n < 0 || (n && (!cells || !rate))) return W2B_EINVAL;
+    StepArgs A;
+    if (!handle_args(handle, &A)) return W2B_EINVAL;
+    if (n) source_runs_kernel<<<SRC_BLOCKS, SRC_THREADS, 0, (cudaStream_t)stream>>>(A, n, cells, rate);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        fprintf(stderr, "libwadi_b200: w2b_source_runs: %s\n", cudaGetErrorString(e));
+        return W2B_ECUDA;
+    }
+    return W2B_OK;
+}
+
 int32_t w2b_storage(void* handle, int64_t n, const int32_t* cells, double* partial, double* out, void* stream) {
     if (!handle || n < 0 || (n && !cells) || !partial || !out) return W2B_EINVAL;
-    float *h = nullptr, *res = nullptr;
-    if (w2b_field_ptr(handle, W2B_H, &h) != W2B_OK || w2b_field_ptr(handle, W2B_RES, &res) != W2B_OK)
-        return W2B_EINVAL;
-    float dx = 0.0f;
-    if (w2b_cell_size(handle, &dx) != W2B_OK) return W2B_EINVAL;
+    StepArgs A;
+    if (!handle_args(handle, &A)) return W2B_EINVAL;
     cudaStream_t s = (cudaStream_t)stream;
-    storage_kernel<<<SRC_BLOCKS, SRC_THREADS, 0, s>>>(n, cells, h, res, partial);
-    finish_kernel<<<1, SRC_THREADS, 0, s>>>(partial, SRC_BLOCKS, (double)dx * (double)dx, out);
+    storage_kernel<<<SRC_BLOCKS, SRC_THREADS, 0, s>>>(A, n, cells, partial);
+    finish_kernel<<<1, SRC_THREADS, 0, s>>>(partial, SRC_BLOCKS, 1.0, out);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         fprintf(stderr, "libwadi_b200: w2b_storage: %s\n", cudaGetErrorString(e));

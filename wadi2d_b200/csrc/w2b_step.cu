@@ -79,18 +79,18 @@ __device__ __forceinline__ void face_a(const float* sm, int b, int local, const 
 // outputs and wave speed (faces.cu:43-44, :52-63, :102-145). Returns the wave speed.
 template <int AX>
 __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int k, const StepArgs& A, int t,
-                                         const FaceA& F, float dt, int want_wave, const float* rowc) {
+                                         const FaceA& F, float dt, float dx, int want_wave, const float* rowc, int p) {
     constexpr int S = AX == 0 ? 1 : BOXW;
     constexpr int PP = AX == 0 ? BOXW : 1;
     const W2BParams& P = A.P;
     if (!F.live) {
-        A.u_next[AX][k] = 0.0f;
-        A.m_next[AX][k] = 0.0f;
+        A.uu[AX][1 - p][k] = 0.0f;
+        A.mm[AX][1 - p][k] = 0.0f;
         A.q1[AX][k] = 0.0f;
         return 0.0f;
     }
     const float ZERO = 0.0f, HALF = 0.5f, ONE = 1.0f;
-    const float dx = P.dx, span = dx;
+    const float span = dx;
     const float* H = sm + F_H * BOX;
     const float* U = sm + (AX == 0 ? F_U : F_V) * BOX;
     const float* VP = sm + (AX == 0 ? F_V : F_U) * BOX;
@@ -207,8 +207,8 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
             un = qn / fmax32(area * rho, 1e-12f);
         }
     }
-    A.u_next[AX][k] = un;
-    A.m_next[AX][k] = abar * un;
+    A.uu[AX][1 - p][k] = un;
+    A.mm[AX][1 - p][k] = abar * un;
     A.q1[AX][k] = qn;
     if (!want_wave) return ZERO;
     if (not_finite(un)) return 1e30f;
@@ -249,17 +249,14 @@ __device__ __forceinline__ float block_max(float v, float* red) {
 // Each CTA (16 warps, a warp a tile row, two rows a warp) stages a tile with TMA: nine 40 x 36 state boxes, the two
 // momenta, and the tile's twelve static face scalars as bulk copies; the per-tile wave maxima are reduced at the end
 // by the last CTA to finish. p is the parity of the ping-pong halves.
-__global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_constant__ TMaps M, StepArgs A, int p) {
+__global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_constant__ TMaps M, StepArgs A) {
     extern __shared__ __align__(128) float sm[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ float red[32];
     __shared__ float rowc[2 * 64 + 1];
-    __shared__ bool last;
     Ctl* ctl = A.ctl;
-    if (!ctl->run) return;
+    if (!(ctl->any & ANY_RUN)) return;
     const int nact = ctl->nact;
-    const float dt = ctl->dtf;
-    const int want_wave = ctl->want_wave;
     const int tid = threadIdx.x;
     if (tid == 0) {
         mbar_init(&bar, 1);
@@ -277,17 +274,23 @@ __global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_co
         rowc[2 * tid] = 1.0f - c * c;
     }
     __syncthreads();
-    const uint32_t bytes = (uint32_t)((NBOX - (want_wave ? 0 : 1)) * BOX + 14 * TILE2) * 4u;
     const float* statics[12] = {A.fl[0], A.fr[0], A.gl[0], A.gr[0], A.ef[0], A.cw[0],
                                 A.fl[1], A.fr[1], A.gl[1], A.gr[1], A.ef[1], A.cw[1]};
     uint32_t phase = 0;
     const int lane = tid & 31, warp = tid >> 5;
     for (int a = blockIdx.x; a < nact; a += gridDim.x) {
         const int t = A.active[a];
+        const int run = A.tile_run[t];
+        const int flags = A.R.flags[run];
+        if (!(flags & F_RUN)) continue;  // the tile's run has finished: uniform over the CTA
+        const float dt = A.R.dtf[run];
+        const float dx = A.R.dx[run];
+        const int want_wave = (flags & F_WAVE) != 0;
+        const int p = A.R.parity[run];
         const int tj = A.tiles[2 * t], ti = A.tiles[2 * t + 1];
         if (tid == 0) {
             fence_proxy_async();
-            mbar_expect_tx(&bar, bytes);
+            mbar_expect_tx(&bar, (uint32_t)((NBOX - (want_wave ? 0 : 1)) * BOX + 14 * TILE2) * 4u);
             const int x0 = ti * TILE + GX - 4, y0 = tj * TILE + GY - 2;
             tma_load_2d(sm + F_D * BOX, &M.d, x0, y0, &bar);
             tma_load_2d(sm + F_H * BOX, &M.h[p], x0, y0, &bar);
@@ -321,33 +324,21 @@ __global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_co
             FaceA fx, fy;
             face_a<0>(sm, b, local, A, t, fx);
             face_a<1>(sm, b, local, A, t, fy);
-            const float wx = face_bc<0>(sm, b, local, k, A, t, fx, dt, want_wave, rowc);
-            const float wy = face_bc<1>(sm, b, local, k, A, t, fy, dt, want_wave, rowc);
+            const float wx = face_bc<0>(sm, b, local, k, A, t, fx, dt, dx, want_wave, rowc, p);
+            const float wy = face_bc<1>(sm, b, local, k, A, t, fy, dt, dx, want_wave, rowc, p);
             wmax = fmax32(wmax, fmax32(wx, wy));
         }
         if (want_wave) {
+            // the tile's wave, and the run's maximum (wadi2d/solver/gpu/kernels/common.cuh:93-96: positive floats
+            // order like their bit patterns, so the integer maximum is the float maximum)
             const float bm = block_max(wmax, red);
-            if (tid == 0) A.wave[t] = bm;
+            if (tid == 0) {
+                A.wave[t] = bm;
+                atomicMax(A.R.wave_bits + run, __float_as_uint(bm));
+            }
         } else {
             __syncthreads();
         }
-    }
-    if (!want_wave) return;
-    // single-pass grid reduction: the last CTA to finish reduces the per-tile maxima (no CTA waits on another)
-    if (tid == 0) {
-        __threadfence();
-        const unsigned v = atomicAdd(&ctl->ticket, 1u);
-        last = (v == gridDim.x - 1);
-    }
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    float w = 0.0f;
-    for (int a = tid; a < nact; a += blockDim.x) w = fmax32(w, __ldcg(A.wave + A.active[a]));
-    const float bm = block_max(w, red);
-    if (tid == 0) {
-        ctl->wave_max = bm;
-        ctl->ticket = 0u;
     }
 }
 
@@ -380,8 +371,8 @@ int faces_occupancy() {
     return occ;
 }
 
-void launch_faces(const TMaps& M, const StepArgs& A, int p, int grid, cudaStream_t s) {
-    faces_kernel<<<grid, FACES_THREADS, FACES_SMEM, s>>>(M, A, p);
+void launch_faces(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s) {
+    faces_kernel<<<grid, FACES_THREADS, FACES_SMEM, s>>>(M, A);
 }
 
 // ------------------------------------------------------------------ update pass
@@ -389,8 +380,9 @@ void launch_faces(const TMaps& M, const StepArgs& A, int p, int grid, cudaStream
 __device__ __forceinline__ float scaled(float q, float rl, float rr) { return q * (q > 0.0f ? rl : rr); }
 
 // Envelope of one own cell, wadi2d/engine/maxima.py:75-92 (the CPU twin forms the centre speed in float64).
+// un, vn: the face velocities after the step.
 __device__ __forceinline__ void envelope(const StepArgs& A, int fid, int k, float dk, float hk, float time,
-                                         float arrive, float deep) {
+                                         float arrive, float deep, const float* un, const float* vn) {
     float* __restrict__ dmax = A.env[0];
     float* __restrict__ hmax = A.env[1];
     float* __restrict__ smax = A.env[2];
@@ -399,8 +391,8 @@ __device__ __forceinline__ void envelope(const StepArgs& A, int fid, int k, floa
     dmax[fid] = fmax32(dmax[fid], dk);
     hmax[fid] = fmax32(hmax[fid], hk);
     if (dk > deep) {
-        const double uc = 0.5 * (double)(A.u_next[0][k] + A.u_next[0][k + 1]);
-        const double vc = 0.5 * (double)(A.u_next[1][k] + A.u_next[1][k + A.px]);
+        const double uc = 0.5 * (double)(un[k] + un[k + 1]);
+        const double vc = 0.5 * (double)(vn[k] + vn[k + A.px]);
         const double s = sqrt(uc * uc + vc * vc);
         const double sm = (double)smax[fid];
         smax[fid] = (float)(sm >= s ? sm : s);
@@ -424,18 +416,13 @@ constexpr int UPDATE_THREADS = 256;
 // discharges and old depth with their ring, its residual, source and Hc; r of the tile and its one-cell ring is
 // formed in shared memory; then each thread takes its four cells through continuity, issues their four level-table
 // loads together, and finishes the level, the wet share, the wet flag and, on envelope steps, the envelope.
-__global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_constant__ TMaps M, StepArgs A, int p) {
+__global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_constant__ TMaps M, StepArgs A) {
     extern __shared__ __align__(128) float sm[];
     __shared__ __align__(8) uint64_t bar;
     Ctl* ctl = A.ctl;
-    if (!ctl->run) return;
+    if (!(ctl->any & ANY_RUN)) return;
     const int nact = ctl->nact;
-    const float dt = ctl->dtf;
-    const int want_plan = ctl->want_wave;
-    const int want_wet = ctl->want_wet;
-    const int want_max = ctl->want_max;
-    const float time = ctl->max_time, arrive = ctl->arrive, deep = ctl->deep;
-    const float area = A.area;
+    const float arrive = ctl->arrive, deep = ctl->deep;
     const int px = A.px;
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     const int rows = A.rows, last = rows - 1;
@@ -455,6 +442,18 @@ __global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_con
     float* rs = sm + U_R;
     for (int a = blockIdx.x; a < nact; a += gridDim.x) {
         const int t = A.active[a];
+        const int run = A.tile_run[t];
+        const int flags = A.R.flags[run];
+        if (!(flags & F_RUN)) continue;  // uniform over the CTA
+        const float dt = A.R.dtf[run];
+        const float dxr = A.R.dx[run];
+        const float area = dxr * dxr;
+        const int want_plan = (flags & F_WAVE) != 0;
+        const int want_wet = (flags & F_WET) != 0;
+        const int want_max = (flags & F_MAX) != 0;
+        const float time = A.R.max_time[run];
+        const int p = A.R.parity[run];
+        float* __restrict__ h_next = A.hh[1 - p];
         const int tj = A.tiles[2 * t], ti = A.tiles[2 * t + 1];
         if (tid == 0) {
             fence_proxy_async();
@@ -508,7 +507,7 @@ __global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_con
             const float total = h0 + inc;
             hn[c] = fmax32(total, 0.0f);
             A.res[k] = total > 0.0f ? inc - (total - h0) : 0.0f;
-            A.h_next[k] = hn[c];
+            h_next[k] = hn[c];
             // the level table's row (common.cuh cell_level): the top row above Hc, none where Hc <= 0
             const float hcv = HC[local];
             if (hcv <= 0.0f) {
@@ -557,7 +556,7 @@ __global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_con
             if (want_plan) A.om[k] = om;
             any |= h > 0.0f;
             if (want_max && !((A.bmark[t * TILE + jj] >> ii) & 1u))
-                envelope(A, t * TILE2 + local, k, dk, h, time, arrive, deep);
+                envelope(A, t * TILE2 + local, k, dk, h, time, arrive, deep, A.uu[0][1 - p], A.uu[1][1 - p]);
         }
         if (want_wet) {
             const int w = __syncthreads_or(any);
@@ -578,107 +577,123 @@ int update_occupancy() {
     return occ;
 }
 
-void launch_update(const TMaps& M, const StepArgs& A, int p, int grid, cudaStream_t s) {
-    update_kernel<<<grid, dim3(32, 8), UPDATE_SMEM, s>>>(M, A, p);
+void launch_update(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s) {
+    update_kernel<<<grid, dim3(32, 8), UPDATE_SMEM, s>>>(M, A);
 }
 
 // ------------------------------------------------------------------ boundary, tally, control (one CTA)
 
-__device__ __forceinline__ int fid_of_native(const StepArgs& A, int k) {
-    const int j = k / A.px - GY;
-    const int i = k - (j + GY) * A.px - GX;
-    const int t = A.tile_of[(j / TILE) * A.ntx + (i / TILE)];
-    return t * TILE2 + (j % TILE) * TILE + (i % TILE);
-}
-
+// Boundary cells of every running run (wadi2d/solver/gpu/kernels/cells.cu:95-111), their envelope entries after the
+// overwrite, and, in the device loop (control = 1), the FP64 tally of every step and each run's clock after its step
+// (wadi2d/solver/stepper.py:113-124). One CTA.
 __global__ void boundary_kernel(StepArgs A, int control) {
     Ctl* ctl = A.ctl;
-    if (!ctl->run) return;
+    if (!(ctl->any & ANY_RUN)) return;
+    const RunTab& R = A.R;
     const int tid = threadIdx.x;
     for (int m = tid; m < A.nb; m += blockDim.x) {
         const int k = A.bcell[m];
+        const int run = A.tile_run[tile_of_native(A, k)];
+        if (!(R.flags[run] & F_RUN)) continue;
+        float* h_next = A.hh[1 - R.parity[run]];
         const int kind = A.bkind[m];
         if (kind == 0) {
-            A.h_next[k] = A.bh0[m];
+            h_next[k] = A.bh0[m];
             A.d[k] = A.bd0[m];
         } else if (kind == 1) {
-            A.h_next[k] = 0.0f;
+            h_next[k] = 0.0f;
             A.d[k] = 0.0f;
         } else {
             const int r = A.bref[m];
-            A.h_next[k] = A.h_next[r];
+            h_next[k] = h_next[r];
             A.d[k] = fmax32(A.d[r] + A.bd0[m], 0.0f);
         }
     }
     __syncthreads();
-    if (ctl->want_max) {
-        for (int m = tid; m < A.nb; m += blockDim.x) {
-            const int k = A.bcell[m];
-            envelope(A, fid_of_native(A, k), k, A.d[k], A.h_next[k], ctl->max_time, ctl->arrive, ctl->deep);
-        }
-    }
-    if (control) {
-        const double dtt = ctl->dt_tally;
-        for (int m = tid; m < A.ntally; m += blockDim.x) {
-            const float qv = A.taxis[m] ? A.q[1][A.tface[m]] : A.q[0][A.tface[m]];
-            A.ttotal[m] += dtt * (double)(A.tsign[m] * qv);
-        }
+    for (int m = tid; m < A.nb; m += blockDim.x) {
+        const int k = A.bcell[m];
+        const int run = A.tile_run[tile_of_native(A, k)];
+        const int n = 1 - R.parity[run];
+        if ((R.flags[run] & (F_RUN | F_MAX)) == (F_RUN | F_MAX))
+            envelope(A, fid_of_native(A, k), k, A.d[k], A.hh[n][k], R.max_time[run], ctl->arrive, ctl->deep,
+                     A.uu[0][n], A.uu[1][n]);
     }
     if (!control) return;
     __syncthreads();
-    if (tid != 0) return;
-    // the stepper's bookkeeping after a step, wadi2d/solver/stepper.py:113-124
-    ctl->t = ctl->t + ctl->dt_step;
-    ctl->nsteps += 1;
-    ctl->steps_run += 1;
-    if (ctl->want_wave) {
-        const double w = (double)ctl->wave_max;
-        if (!isfinite(w)) {
-            ctl->status = W2B_ENONFINITE;
-        } else {
-            const double lim = ctl->cfl * ctl->dx / (ctl->wave_floor > w ? ctl->wave_floor : w);
-            ctl->dt = ctl->dt_max < lim ? ctl->dt_max : lim;
-            if (ctl->dt < ctl->dt_min) ctl->status = W2B_EDTMIN;
+    for (int m = tid; m < A.ntally; m += blockDim.x) {
+        const int face = A.tface[m];
+        const int run = A.tile_run[tile_of_native(A, face)];
+        if (!(R.flags[run] & F_RUN)) continue;
+        const float qv = A.taxis[m] ? A.q[1][face] : A.q[0][face];
+        A.ttotal[m] += R.dt_tally[run] * (double)(A.tsign[m] * qv);
+    }
+    for (int r = tid; r < A.nruns; r += blockDim.x) {
+        if (!(R.flags[r] & F_RUN)) continue;
+        R.parity[r] ^= 1;
+        R.t[r] = R.t[r] + R.dt_step[r];
+        R.nsteps[r] += 1;
+        R.steps_run[r] += 1;
+        if (R.flags[r] & F_WAVE) {
+            const double w = (double)__uint_as_float(R.wave_bits[r]);
+            if (!isfinite(w)) {
+                R.status[r] = W2B_ENONFINITE;
+            } else {
+                const double lim = ctl->cfl * (double)R.dx[r] / (ctl->wave_floor > w ? ctl->wave_floor : w);
+                R.dt[r] = ctl->dt_max < lim ? ctl->dt_max : lim;
+                if (R.dt[r] < ctl->dt_min) R.status[r] = W2B_EDTMIN;
+            }
         }
     }
 }
 
-// Before a step of the device loop: the loop test and the step's settings, wadi2d/solver/stepper.py:106-111.
-__global__ void prestep_kernel(Ctl* ctl) {
-    if (ctl->status != 0 || !(ctl->t < ctl->t_end - 1e-9) || ctl->steps_run >= ctl->max_steps) {
-        ctl->run = 0;
-        return;
+// Before a step of the device loop, for each run: the loop test and the step's settings
+// (wadi2d/solver/stepper.py:106-111). One CTA; ctl->any gathers the runs' flags.
+__global__ void prestep_kernel(StepArgs A) {
+    Ctl* ctl = A.ctl;
+    const RunTab& R = A.R;
+    __shared__ uint32_t any;
+    if (threadIdx.x == 0) any = 0u;
+    __syncthreads();
+    uint32_t mine = 0u;
+    for (int r = threadIdx.x; r < A.nruns; r += blockDim.x) {
+        if (ctl->status != 0 || R.status[r] != 0 || !(R.t[r] < R.t_end[r] - 1e-9) || R.steps_run[r] >= R.max_steps[r]) {
+            R.flags[r] = 0;
+            continue;
+        }
+        const int refresh = R.refresh_due[r] || (R.nsteps[r] % ctl->dt_every == 0);
+        R.refresh_due[r] = 0;
+        const int activate = (int)(R.nsteps[r] % ctl->active_every == 0);
+        double dt = R.dt[r];
+        const double rest = R.t_end[r] - R.t[r];
+        if (rest < dt) dt = rest;
+        if (ctl->dt_max < dt) dt = ctl->dt_max;
+        R.dt_step[r] = dt;
+        R.dtf[r] = (float)dt;
+        const double t_new = R.t[r] + dt;
+        R.dt_tally[r] = t_new - R.t[r];
+        R.max_time[r] = (float)t_new;
+        const int want_max = ctl->max_every > 0 && ((R.nsteps[r] + 1) % ctl->max_every == 0);
+        const int act = activate && ctl->adaptive;
+        R.flags[r] = F_RUN | (refresh ? F_WAVE : 0) | (activate ? F_WET : 0) | (want_max ? F_MAX : 0) | (act ? F_ACT : 0);
+        if (refresh) R.wave_bits[r] = 0u;
+        mine |= ANY_RUN | (refresh ? ANY_WAVE : 0u) | (act ? ANY_ACT : 0u);
     }
-    ctl->run = 1;
-    const int refresh = ctl->refresh_due || (ctl->nsteps % ctl->dt_every == 0);
-    ctl->refresh_due = 0;
-    const int activate = (int)(ctl->nsteps % ctl->active_every == 0);
-    double dt = ctl->dt;
-    const double rest = ctl->t_end - ctl->t;
-    if (rest < dt) dt = rest;
-    if (ctl->dt_max < dt) dt = ctl->dt_max;
-    ctl->dt_step = dt;
-    ctl->dtf = (float)dt;
-    ctl->want_wave = refresh;
-    ctl->want_wet = activate;
-    ctl->activate = activate && ctl->adaptive;
-    const double t_new = ctl->t + dt;
-    ctl->dt_tally = t_new - ctl->t;
-    ctl->max_time = (float)t_new;
-    ctl->want_max = ctl->max_every > 0 && ((ctl->nsteps + 1) % ctl->max_every == 0);
-    ctl->ticket = 0u;
+    if (mine) atomicOr(&any, mine);
+    __syncthreads();
+    if (threadIdx.x == 0) ctl->any = any;
 }
 
-// A host-driven step (the reference backend's step(dt, want_wave, want_wet)).
-__global__ void setstep_kernel(Ctl* ctl, float dtf, int want_wave, int want_wet, int nact) {
-    ctl->run = 1;
-    ctl->dtf = dtf;
-    ctl->want_wave = want_wave;
-    ctl->want_wet = want_wet;
-    ctl->want_max = 0;
+// The end of a host-driven step of run 0: the swap of the ping-pong pairs (wadi2d/solver/gpu/backend.py:185-188).
+__global__ void endstep_kernel(StepArgs A) { A.R.parity[0] ^= 1; }
+
+// A host-driven step of run 0 (the reference backend's step(dt, want_wave, want_wet)).
+__global__ void setstep_kernel(StepArgs A, float dtf, int want_wave, int want_wet, int nact) {
+    Ctl* ctl = A.ctl;
     ctl->nact = nact;
-    ctl->ticket = 0u;
-    if (want_wave) ctl->wave_max = 0.0f;
+    ctl->any = ANY_RUN | (want_wave ? ANY_WAVE : 0u);
+    A.R.dtf[0] = dtf;
+    A.R.flags[0] = F_RUN | (want_wave ? F_WAVE : 0) | (want_wet ? F_WET : 0);
+    if (want_wave) A.R.wave_bits[0] = 0u;
 }
 
 // ------------------------------------------------------------------ active-list rebuild (one CTA of 1024)
@@ -708,12 +723,13 @@ __device__ __forceinline__ int block_scan(int flag, int* warp_sums, int* total) 
     return before;
 }
 
-// rebuild_active(check=True), wadi2d/solver/stepper.py:56-92, when ctl->activate: wet or kept tiles and their
+// rebuild_active(check=True), wadi2d/solver/stepper.py:56-92, for the runs that rebuild at this step: wet or kept
+// tiles and their
 // eight neighbours are active; a tile sleeps after SLEEP_CHECKS checks in a row that did not want it; tiles that
 // join the list are listed in woken for their wet share to be written.
 __global__ void __launch_bounds__(1024) activity_kernel(StepArgs A) {
     Ctl* ctl = A.ctl;
-    if (!ctl->run || !ctl->activate) return;
+    if (!(ctl->any & ANY_ACT)) return;
     const int nt = A.ntiles;
     int* wet_eff = A.scratch;
     int* flags = A.scratch + nt;
@@ -724,9 +740,13 @@ __global__ void __launch_bounds__(1024) activity_kernel(StepArgs A) {
             flags[0] = 0;
             continue;
         }
+        const int cur = A.is_act[t];
+        if (!(A.R.flags[A.tile_run[t]] & F_ACT)) {  // this tile's run does not rebuild at this step
+            flags[t] = cur;
+            continue;
+        }
         int act = wet_eff[t];
         for (int n = 0; n < 8; ++n) act |= wet_eff[A.nbr[8 * t + n]];
-        const int cur = A.is_act[t];
         if (act)
             A.idle[t] = 0;
         else
@@ -755,12 +775,12 @@ __global__ void __launch_bounds__(1024) activity_kernel(StepArgs A) {
     }
 }
 
-// refresh_plan of the listed tiles (wadi2d/solver/gpu/kernels/cells.cu:66-78) from the mean depth h. count < 0:
+// refresh_plan of the listed tiles (wadi2d/solver/gpu/kernels/cells.cu:66-78) from the current mean depth. count < 0:
 // the tiles the device loop's rebuild woke (ctl->nwoken).
-__global__ void __launch_bounds__(256) plan_kernel(StepArgs A, const int32_t* list, int count, const float* h) {
+__global__ void __launch_bounds__(256) plan_kernel(StepArgs A, const int32_t* list, int count) {
     Ctl* ctl = A.ctl;
     if (count < 0) {
-        if (!ctl->run || !ctl->activate) return;
+        if (!(ctl->any & ANY_ACT)) return;
         count = ctl->nwoken;
     }
     for (int a = blockIdx.x; a < count; a += gridDim.x) {
@@ -768,6 +788,7 @@ __global__ void __launch_bounds__(256) plan_kernel(StepArgs A, const int32_t* li
         const int tj = A.tiles[2 * t], ti = A.tiles[2 * t + 1];
         const int base = (tj * TILE + GY) * A.px + ti * TILE + GX;
         const float2* pairs_t = A.dtab2 + (size_t)t * (A.rows - 1) * TILE2;
+        const float* h = A.hh[A.R.parity[A.tile_run[t]]];
         for (int c = 0; c < 4; ++c) {
             const int jj = threadIdx.y * 4 + c, ii = threadIdx.x;
             const int local = jj * TILE + ii;
@@ -777,8 +798,8 @@ __global__ void __launch_bounds__(256) plan_kernel(StepArgs A, const int32_t* li
     }
 }
 
-// Maxima.update over the active tiles, host-driven (wadi2d/engine/maxima.py:118-130). A's current halves are the
-// state after the step, so u_next here must point at the current u and v.
+// Maxima.update over the active tiles, host-driven (wadi2d/engine/maxima.py:118-130): the current halves are the
+// state after the step.
 __global__ void __launch_bounds__(256) maxima_kernel(StepArgs A, float time, float arrive, float deep, int nact) {
     for (int a = blockIdx.x; a < nact; a += gridDim.x) {
         const int t = A.active[a];
@@ -787,7 +808,8 @@ __global__ void __launch_bounds__(256) maxima_kernel(StepArgs A, float time, flo
         for (int c = 0; c < 4; ++c) {
             const int jj = threadIdx.y * 4 + c, ii = threadIdx.x;
             const int k = base + jj * A.px + ii;
-            envelope(A, t * TILE2 + jj * TILE + ii, k, A.d[k], A.h[k], time, arrive, deep);
+            const int pc = A.R.parity[A.tile_run[t]];
+            envelope(A, t * TILE2 + jj * TILE + ii, k, A.d[k], A.hh[pc][k], time, arrive, deep, A.uu[0][pc], A.uu[1][pc]);
         }
     }
 }

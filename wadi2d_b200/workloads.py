@@ -200,3 +200,38 @@ def catchment(n: int = 4096, dx: float = 30.0, k: int = 4, seed: int = 7, relief
     rain = field[np.ix_(cc, cc)]
     rain[~domain.cpu().numpy()] = 0.0
     return Catchment(n, dx, k, zp, 0.035, outfalls, rain, 12 * 3600.0, 36 * 3600.0, 10.0, 2.0)
+
+
+@dataclass(frozen=True)
+class EnsembleRun:
+    """One run of configuration 4: a seeded fractal fan (``catchment`` at this side, cell size and relief) under a
+    uniform storm of its own."""
+
+    side: int
+    dx: float
+    seed: int
+    relief: float
+    depth_mm: float
+    duration_min: float
+    arf: float
+
+    def storm(self):
+        from wadi2d_b200.forcing import GivenFactor, UniformStorm
+
+        return UniformStorm(self.depth_mm, self.duration_min, arf=GivenFactor(self.arf))
+
+
+def ensemble(nruns: int = 64, seed: int = 11, side_min: int = 256, side_max: int = 2048) -> list[EnsembleRun]:
+    """Configuration 4: square domains with sides log-uniform in [side_min, side_max] cells at 10-30 m (4 x 4
+    pixels a cell), fans with about 3 % of relief over their length, storm durations log-uniform over 1-24 h, depths
+    uniform over 20-200 mm, ARF factors uniform over 0.6-1.0."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for r in range(nruns):
+        side = int(round(np.exp(rng.uniform(np.log(side_min), np.log(side_max)))))
+        dx = float(np.round(rng.uniform(10.0, 30.0), 2))
+        dur = float(np.round(np.exp(rng.uniform(np.log(60.0), np.log(1440.0))), 1))
+        depth = float(np.round(rng.uniform(20.0, 200.0), 1))
+        arf = float(np.round(rng.uniform(0.6, 1.0), 3))
+        out.append(EnsembleRun(side, dx, 1000 + r, 0.03 * side * dx, depth, dur, arf))
+    return out

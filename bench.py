@@ -302,76 +302,116 @@ def ensemble_inputs(spec, dev):
 def ensemble_run(args) -> None:
     """Configuration 4: 64 runs of uneven size, cell size and storm (uniform rain, each run its own depth, duration
     and ARF factor), each from dry ground to the end of its storm plus a recession, the envelope every 4 steps and
-    the FP64 outfall tally every step. Timed twice on one GPU: as one batch (w2b_advance_runs) and one run after
-    another (the plain per-run device loop). Both give every run the same steps and the same envelope."""
+    the FP64 outfall tally every step. Timed twice: as one batch (w2b_advance_runs) and one run after another (the
+    plain per-run device loop); both give every run the same steps and the same envelope. Under torchrun the runs
+    are split over the ranks by estimated cell-steps (no exchange while they step); the times are CUDA events, the
+    max over ranks, and rank 0 gathers the per-run records."""
     import torch
+    import torch.distributed as dist
 
-    from wadi2d_b200 import workloads
+    from wadi2d_b200 import sweep, workloads
     from wadi2d_b200.batch import Batch
     from wadi2d_b200.config import Numerics
     from wadi2d_b200.maxima import Maxima, Tally
     from wadi2d_b200.model import Model
     from wadi2d_b200.run import DeviceRain, run_windows
 
-    dev = torch.device("cuda", 0)
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=900))
     specs = workloads.ensemble(args.runs, side_max=args.side_max)
+    t_all = np.array([(sp.duration_min + args.recession_min) * 60.0 * args.time_scale for sp in specs])
+    costs = [sweep.run_cost(sp.side**2, t_all[r], sp.dx) for r, sp in enumerate(specs)]
+    mine = sweep.partition(costs, world)[rank]
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn):
+        """fn() between CUDA events on the current stream; the max over ranks, seconds."""
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        if world > 1:
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        sec = e0.elapsed_time(e1) / 1e3
+        if world > 1:
+            t = torch.tensor([sec], device=dev, dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            sec = float(t.item())
+        return out, sec
+
     t0 = time.perf_counter()
-    inputs = [ensemble_inputs(sp, dev) for sp in specs]
+    inputs = [ensemble_inputs(specs[r], dev) for r in mine]
     torch.cuda.synchronize(dev)
     setup = time.perf_counter() - t0
     num = Numerics()
-    t_end = np.array([(sp.duration_min + args.recession_min) * 60.0 * args.time_scale for sp in specs])
-    storms = [sp.storm() for sp in specs]
+    t_end = t_all[mine]
+    storms = [specs[r].storm() for r in mine]
     cells = np.array([int(i[0].mask.sum()) for i in inputs], np.float64)
-    plain = None
+    records = {r: {"side": specs[r].side, "cells": int(cells[n]), "simulated_h": float(t_end[n]) / 3600.0}
+               for n, r in enumerate(mine)}  # fmt: skip
+    plain_s = None
     if not args.skip_plain:
-        steps, peak, walls = [], [], []
-        for r, (grid, tables, bc, interior, tspec) in enumerate(inputs):
-            m = Model(tables, num)
-            m.set_boundary(bc)
-            m.set_depth(np.zeros(grid.shape))
-            tally = Tally(m, *tspec)
-            maxima = Maxima(m, 0.1, 0.05, every=4)
-            rain = DeviceRain(m, storms[r], interior)
-            torch.cuda.synchronize(dev)
-            w0 = time.perf_counter()
-            run_windows(m, t_end[r], rain=rain, window=30.0, maxima=maxima, tally=tally)
-            torch.cuda.synchronize(dev)
-            walls.append(time.perf_counter() - w0)
-            steps.append(m.stepper.nsteps)
-            peak.append(float(maxima.fields()["depth"].max()))
-            del m, tally, maxima, rain
-        wall = float(sum(walls))
-        plain = {"wall_s": wall, "runs_per_h": 3600.0 * len(specs) / wall,
-                 "cell_steps_per_s": float(np.dot(cells, steps)) / wall, "steps": steps, "peak_depth": peak}  # fmt: skip
+
+        def plain_sweep():
+            for n, (grid, tables, bc, interior, tspec) in enumerate(inputs):
+                m = Model(tables, num)
+                m.set_boundary(bc)
+                m.set_depth(np.zeros(grid.shape))
+                tally = Tally(m, *tspec)
+                maxima = Maxima(m, 0.1, 0.05, every=4)
+                rain = DeviceRain(m, storms[n], interior)
+                run_windows(m, t_end[n], rain=rain, window=30.0, maxima=maxima, tally=tally)
+                rec = records[mine[n]]
+                rec["plain_steps"] = int(m.stepper.nsteps)
+                rec["plain_peak_depth"] = float(maxima.fields()["depth"].max())
+                del m, tally, maxima, rain
+
+        _, plain_s = timed(plain_sweep)
     b0 = time.perf_counter()
     B = Batch([i[0] for i in inputs], [i[1] for i in inputs], num)
     B.set_boundary([i[2] for i in inputs])
     B.set_depth([np.zeros(i[0].shape) for i in inputs])
     B.set_tally([i[4] for i in inputs])
     B.reset_envelope()
-    rc = [B.native_of(r, i[3]) for r, i in enumerate(inputs)]
+    rc = [B.native_of(n, i[3]) for n, i in enumerate(inputs)]
     torch.cuda.synchronize(dev)
     pack_s = time.perf_counter() - b0
-    w0 = time.perf_counter()
-    books = B.run_windows(t_end, storms, window=30.0, max_every=4, cells=rc)
-    torch.cuda.synchronize(dev)
-    wall = time.perf_counter() - w0
-    bsteps = [int(x) for x in B.nsteps]
-    bpeak = [float(B.envelope(r)["depth"].max()) for r in range(len(specs))]
-    batch = {"wall_s": wall, "pack_s": pack_s, "runs_per_h": 3600.0 * len(specs) / wall,
-             "cell_steps_per_s": float(np.dot(cells, bsteps)) / wall, "loop_steps": int(max(bsteps)),
-             "tiles": int(B.grid.ntiles - 1)}  # fmt: skip
-    line = {
-        "run": "configuration 4 ensemble", "runs": len(specs), "cells": int(cells.sum()),
-        "sides": [sp.side for sp in specs], "simulated_h": [float(t) / 3600.0 for t in t_end],
-        "setup_s": setup, "batch": batch, "plain": plain,
-        "same_steps": None if plain is None else plain["steps"] == bsteps,
-        "same_peak_depth": None if plain is None else plain["peak_depth"] == bpeak,
-        "speedup": None if plain is None else plain["wall_s"] / wall,
-        "rain_m3": float(sum(b.rain for b in books)), "outflow_m3": float(sum(b.outflow for b in books)),
-    }  # fmt: skip
-    print(json.dumps(line), flush=True)
+    books, batch_s = timed(lambda: B.run_windows(t_end, storms, window=30.0, max_every=4, cells=rc))
+    for n, r in enumerate(mine):
+        rec = records[r]
+        rec["steps"] = int(B.nsteps[n])
+        rec["peak_depth"] = float(B.envelope(n)["depth"].max())
+        rec["rain_m3"] = books[n].rain
+        rec["outflow_m3"] = books[n].outflow
+    allrec = sweep.gather_results(records, world, rank)
+    if rank == 0:
+        recs = list(allrec.values())
+        cs = float(sum(x["cells"] * x["steps"] for x in recs))
+        line = {
+            "run": "configuration 4 ensemble", "runs": len(recs), "n_gpus": world, "cells": int(sum(x["cells"] for x in recs)),
+            "setup_s_rank0": setup, "pack_s_rank0": pack_s,
+            "batch": {"s": batch_s, "runs_per_h": 3600.0 * len(recs) / batch_s, "cell_steps_per_s": cs / batch_s,
+                      "tiles_rank0": int(B.grid.ntiles - 1), "loop_steps_rank0": int(B.nsteps.max())},
+            "plain": None if plain_s is None else {"s": plain_s, "runs_per_h": 3600.0 * len(recs) / plain_s,
+                                                   "cell_steps_per_s": cs / plain_s},
+            "speedup": None if plain_s is None else plain_s / batch_s,
+            "same_steps": None if plain_s is None else all(x["steps"] == x["plain_steps"] for x in recs),
+            "same_peak_depth": None if plain_s is None else all(x["peak_depth"] == x["plain_peak_depth"] for x in recs),
+            "rain_m3": float(sum(x["rain_m3"] for x in recs)), "outflow_m3": float(sum(x["outflow_m3"] for x in recs)),
+            "imbalance": sweep.imbalance(costs, sweep.partition(costs, world)),
+            "per_run": [[x["side"], round(x["simulated_h"], 3), x["steps"]] for x in recs],
+        }  # fmt: skip
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 def main() -> None:

@@ -91,6 +91,7 @@ typedef struct {
     int32_t *idle;    /* checks in a row a tile was not wanted */
     int32_t *is_act;  /* 1 on active tiles */
     int32_t *woken;   /* tiles that joined the list at the last rebuild */
+    int32_t *work;    /* the device loop's work list: active tiles of the runs still stepping */
     int32_t *scratch; /* 2 * ntiles */
     /* (ntiles, 32) bit per cell: boundary cells, whose envelope entry follows the boundary overwrite */
     uint32_t *bmark;
@@ -166,6 +167,14 @@ int32_t w2b_set_boundary(void* handle, int32_t n, const int32_t* cell, const int
  * total per face in total[n]. Device arrays. */
 int32_t w2b_set_tally(void* handle, int32_t n, const int32_t* face, const int32_t* axis, const float* sign,
                       double* total);
+
+/* Design lines (wadi2d/forcing.py:411-425 for the faces, wadi2d/engine/monitor.py:229-232 for the discharge), taken
+ * every step of the device loop: line l's faces are face[start[l] .. start[l + 1]) (NATIVE index, axis 0 x / 1 y,
+ * sign: +1 or -1, positive to the line's right), all in one run; q[l] = the discharge after the step (m3/s, FP64),
+ * peak[l] = the largest |q[l]| so far and time[l] the time it was reached. Device arrays, kept by the caller;
+ * zero peak[] to start a new search. */
+int32_t w2b_set_lines(void* handle, int32_t nlines, const int32_t* start, const int32_t* face, const int32_t* axis,
+                      const float* sign, double* q, double* peak, double* time);
 
 /* Replaces step (wadi2d/solver/gpu/backend.py:151-188): faces, positivity, update, boundary, then the swap. */
 int32_t w2b_step(void* handle, float dt, int32_t want_wave, int32_t want_wet, void* stream);

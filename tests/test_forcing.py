@@ -74,3 +74,19 @@ def test_open_faces_match_a_direct_count():
     assert yi.size == 0
     assert np.array_equal(np.sort(xi), np.sort(state_index(g, np.arange(1, 7), np.full(6, 7))))
     assert np.all(xs == 1.0)
+
+
+def test_injection_matches_reference_vectors():
+    g = np.load(GOLDEN)
+    bounds = np.concatenate(([0], np.cumsum(g["inj_len"])))
+    for n in range(g["inj_len"].size):
+        times = g["inj_times"][bounds[n] : bounds[n + 1]]
+        flows = g["inj_flows"][bounds[n] : bounds[n + 1]]
+        inj = F.Injection("g", np.arange(5), np.arange(5), 2, times, flows, 0.01)
+        vol = np.array([inj.volume_at(float(t)) for t in g["inj_t"]])
+        assert np.array_equal(vol, g["inj_vol"][n])
+        q = np.array([inj.mean_flow(float(a), float(b)) for a, b in g["inj_windows"]])
+        assert np.array_equal(q, g["inj_q"][n])
+    inj = F.Injection("s", np.arange(5), np.arange(5), 3, g["inj_times"][:3], g["inj_flows"][:3], 0.01)
+    shares = np.stack([inj.share(d) for d in g["inj_depths"]])
+    assert np.array_equal(shares, g["inj_shares"])

@@ -120,3 +120,48 @@ def test_configuration1_full_size_matches_the_oracle_and_balances():
     rain_volume = float(np.float32(rain_rate)) * cells_rained * area * w.rain_s
     bal = F.Balance(rain=rain_volume, outflow=out_g, storage=F.storage(m, interior))
     assert abs(bal.relative) < 1e-6, bal
+
+
+def test_design_lines_take_the_peak_discharge_every_step():
+    from wadi2d_b200.maxima import Lines, faces_across
+
+    w, og, g, tab = c1(64)
+    rows, cols = w.outfall
+    out_ref = np.array([state_index(g, int(j), int(i)) for j, i in zip(rows, cols, strict=True)], np.int32)
+    nb = out_ref.size
+    bc = BoundaryCells(out_ref, np.zeros(nb, np.int32), np.ones(nb, np.int32), np.zeros(nb, np.float32),
+                       np.zeros(nb, np.float32))  # fmt: skip
+    rate = np.zeros(g.shape)
+    rate[1 : 1 + w.ny, 1 : w.nx] = w.rain_mm_h / 3.6e6
+    jj = np.arange(1, 1 + w.ny)
+    lines = [faces_across(g, jj, np.full(jj.size, c), axis=1) for c in (20, 40, 60)]
+    lines.append(faces_across(g, np.full(20, 33), np.arange(22, 42), axis=0, sign=-1.0))
+    t_end = 1800.0
+
+    dev = Model(GridTables.from_dict(g, tab), Numerics(cfl=w.cfl))
+    dev.set_boundary(BoundaryCells(*[np.copy(x) for x in (bc.cell, bc.ref, bc.kind, bc.d0, bc.h0)]))
+    dev.set_source(rate)
+    ln = Lines(dev, lines)
+    dev.run(t_end)
+    q_dev, t_dev = ln.peaks()
+
+    host = Model(GridTables.from_dict(g, tab), Numerics(cfl=w.cfl))
+    host.set_boundary(bc)
+    host.set_source(rate)
+    peak = np.zeros(len(lines))
+    when = np.zeros(len(lines))
+
+    def on_step(st):
+        for n, (xf, xs, yf, ys) in enumerate(lines):
+            q = np.dot(host.read_cells("qx", xf), xs) + np.dot(host.read_cells("qy", yf), ys)
+            if abs(q) > peak[n]:
+                peak[n], when[n] = abs(q), st.t
+
+    host.advance(t_end, on_step)
+    assert dev.stepper.nsteps == host.stepper.nsteps
+    assert np.all(q_dev > 0.0)
+    np.testing.assert_allclose(q_dev, peak, rtol=1e-12)
+    assert np.array_equal(t_dev, when)
+    qn = ln.discharge()
+    xf, xs, yf, ys = lines[1]
+    assert qn[1] == pytest.approx(float(np.dot(dev.read_cells("qx", xf), xs)), rel=1e-12)

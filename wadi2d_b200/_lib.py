@@ -48,7 +48,7 @@ class Buffers(ctypes.Structure):
         + [(n, c_vp * 2) for n in ("fl", "fr", "gl", "gr", "ef", "cw")]
         + [("dtab2", c_vp), ("ftab4", c_vp * 2)]
         + [(n, c_vp) for n in ("tiles", "tile_of", "nbr", "active", "wave", "wet", "keep", "idle", "is_act", "woken",
-                               "scratch", "bmark")]  # fmt: skip
+                               "work", "scratch", "bmark")]  # fmt: skip
         + [("env", c_vp * 5), ("ctl", c_vp), ("runs", c_vp), ("tile_run", c_vp), ("stage", c_vp)]
     )
 
@@ -100,6 +100,7 @@ _SIGNATURES = {
     "w2b_set_run_dx": [c_vp, c_vp, c_i32],
     "w2b_run_halves": [c_vp, c_vp, c_vp],
     "w2b_source_runs": [c_vp, c_i64, c_vp, c_vp, c_vp],
+    "w2b_set_lines": [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
     "w2b_advance_runs": [c_vp, ctypes.POINTER(Stepper), c_vp, c_i64, c_vp, c_vp],
     "w2b_cell_size": [c_vp, ctypes.POINTER(c_f32)],
     "w2b_rain_window": [c_vp, c_vp, c_f64, c_f64, c_f64, c_f64, c_vp, c_vp],

@@ -185,7 +185,7 @@ class B200Backend:
         t["tiles"] = up(g.tiles, torch.int32)
         t["tile_of"] = up(g.tile_of, torch.int32)
         t["nbr"] = up(g.nbr, torch.int32)
-        for n in ("active", "wet", "keep", "idle", "is_act", "woken"):
+        for n in ("active", "wet", "keep", "idle", "is_act", "woken", "work"):
             t[n] = i32(nt)
         t["wave"] = f32(nt)
         t["scratch"] = i32(2 * nt)
@@ -217,7 +217,7 @@ class B200Backend:
             getattr(B, n)[0] = t[n][0].data_ptr()
             getattr(B, n)[1] = t[n][1].data_ptr()
         for n in ("d", "qx", "qy", "qx1", "qy1", "res", "src", "om", "zcx", "zcy", "hc", "dtab2", "tiles", "tile_of",
-                  "nbr", "active", "wave", "wet", "keep", "idle", "is_act", "woken", "scratch", "bmark", "ctl",
+                  "nbr", "active", "wave", "wet", "keep", "idle", "is_act", "woken", "work", "scratch", "bmark", "ctl",
                   "runs", "tile_run", "stage"):  # fmt: skip
             setattr(B, n, t[n].data_ptr())
         for a, ax in enumerate("xy"):

@@ -308,6 +308,26 @@ class Batch:
         self._tally = self.backend.set_tally(np.concatenate(faces), np.concatenate(axis).astype(np.int32),
                                              np.concatenate(sign).astype(np.float32))  # fmt: skip
 
+    def set_lines(self, per_run: list) -> None:
+        """Design lines of each run: a list of (xfaces, xsign, yfaces, ysign) in the run's own state indices (or
+        None). ``line_peaks`` gives each run's peaks in the same order."""
+        from wadi2d_b200.maxima import Lines
+
+        flat, self._line_slices = [], []
+        for r, lines in enumerate(per_run):
+            at = len(flat)
+            for xf, xs, yf, ys in lines or ():
+                flat.append((self.state_index(r, np.asarray(xf, np.int64)), xs,
+                             self.state_index(r, np.asarray(yf, np.int64)), ys))  # fmt: skip
+            self._line_slices.append(slice(at, len(flat)))
+        self.lines = Lines(self, flat)
+
+    def line_peaks(self, r: int) -> tuple[np.ndarray, np.ndarray]:
+        """Run r's design-line peaks |Q| (m3/s) and their times (s)."""
+        q, t = self.lines.peaks()
+        s = self._line_slices[r]
+        return q[s], t[s]
+
     # ------------------------------------------------------------------ the loop
 
     def advance(self, t_end, max_every: int = 0, arrive: float = 0.1, deep: float = 0.05,
@@ -382,7 +402,19 @@ class Batch:
                       b._stream())  # fmt: skip
             if self.stepper.adaptive_active:
                 keep = [run_tiles[r] for r in np.nonzero(falling & live)[0]]
-                self.set_source_tiles(np.concatenate(keep) if keep else np.zeros(0, np.int64))
+                tiles = np.concatenate(keep) if keep else np.zeros(0, np.int64)
+                st = self.stepper
+                if np.all(st.keep_active[tiles]):
+                    # no tile joins the kept set: the host's rebuild (retain) would leave the active list as it is,
+                    # since every device rebuild already took the wet and kept tiles with their neighbours; only the
+                    # kept flags change (they go to the device with the next advance)
+                    self._source_tiles[:] = False
+                    self._source_tiles[tiles] = True
+                    st.keep_active[:] = self._source_tiles
+                    st.keep_active[self.boundary_tiles] = True
+                    st.keep_active[0] = False
+                else:
+                    self.set_source_tiles(tiles)
             self.refresh_due[live] = 1
             self.advance(t1, max_every=max_every, arrive=arrive, deep=deep)
         out = self.tally_volumes()

@@ -24,7 +24,7 @@ __global__ void boundary_kernel(StepArgs A, int control);
 __global__ void prestep_kernel(StepArgs A);
 __global__ void setstep_kernel(StepArgs A, float dtf, int want_wave, int want_wet, int nact);
 __global__ void endstep_kernel(StepArgs A);
-__global__ void activity_kernel(StepArgs A);
+__global__ void activity_kernel(StepArgs A, int only_work);
 __global__ void plan_kernel(StepArgs A, const int32_t* list, int count);
 __global__ void maxima_kernel(StepArgs A, float time, float arrive, float deep, int nact);
 __global__ void tally_kernel(StepArgs A, double dt);
@@ -56,6 +56,10 @@ struct Handle {
     const int32_t *tface = nullptr, *taxis = nullptr;
     const float* tsign = nullptr;
     double* ttotal = nullptr;
+    int nlines = 0;
+    const int32_t *lstart = nullptr, *lface = nullptr, *laxis = nullptr;
+    const float* lsign = nullptr;
+    double *lq = nullptr, *lpeak = nullptr, *ltime = nullptr;
     int sms = 148;
     int step_blocks = 148;   // resident CTAs of the update pass
     int faces_blocks = 296;  // resident CTAs of the face pass
@@ -113,6 +117,8 @@ static StepArgs make_args(const Handle& H) {
     A.idle = H.B.idle;
     A.is_act = H.B.is_act;
     A.woken = H.B.woken;
+    A.work = H.B.work;
+    A.list = H.B.active;  // the host-driven step takes the active list; the device loop its work list
     A.scratch = H.B.scratch;
     for (int e = 0; e < 5; ++e) A.env[e] = H.B.env[e];
     A.bmark = H.B.bmark;
@@ -127,6 +133,14 @@ static StepArgs make_args(const Handle& H) {
     A.taxis = H.taxis;
     A.tsign = H.tsign;
     A.ttotal = H.ttotal;
+    A.nlines = H.nlines;
+    A.lstart = H.lstart;
+    A.lface = H.lface;
+    A.laxis = H.laxis;
+    A.lsign = H.lsign;
+    A.lq = H.lq;
+    A.lpeak = H.lpeak;
+    A.ltime = H.ltime;
     A.ctl = H.ctl();
     A.tile_run = H.B.tile_run;
     A.R = H.R;
@@ -223,14 +237,15 @@ static void drop_graphs(Handle& H) {
 
 // One step of the device loop: every running run advances by one of its own steps.
 static int launch_loop_step(Handle& H, cudaStream_t s) {
-    const StepArgs A = make_args(H);
+    StepArgs A = make_args(H);
+    A.list = A.work;
     const dim3 blk(32, 8);
     const int grid = blocks_for(H, H.g.ntiles - 1);
     prestep_kernel<<<1, 1024, 0, s>>>(A);
     launch_faces(H.tmaps, A, faces_grid(H, H.g.ntiles - 1), s);
     launch_update(H.tmaps, A, grid, s);
     boundary_kernel<<<1, 256, 0, s>>>(A, 1);
-    activity_kernel<<<1, 1024, 0, s>>>(A);
+    activity_kernel<<<1, 1024, 0, s>>>(A, 0);
     plan_kernel<<<grid, blk, 0, s>>>(A, A.woken, -1);
     CKL("loop step");
     return W2B_OK;
@@ -283,7 +298,7 @@ int32_t w2b_ref_to_native(const W2BGridDesc* grid, const int32_t* tiles_host, in
 int32_t w2b_create(const W2BGridDesc* grid, const W2BParams* params, const W2BBuffers* buffers, void** handle) {
     if (!grid || !params || !buffers || !handle) return W2B_EINVAL;
     if (grid->rows < 4 || grid->rows > 64 || grid->nruns < 1) return W2B_EINVAL;
-    if (!buffers->runs || ((uintptr_t)buffers->runs & 255) || !buffers->tile_run) return W2B_EINVAL;
+    if (!buffers->runs || ((uintptr_t)buffers->runs & 255) || !buffers->tile_run || !buffers->work) return W2B_EINVAL;
     Handle* H = new (std::nothrow) Handle();
     if (!H) return W2B_EINVAL;
     H->g = *grid;
@@ -395,6 +410,23 @@ int32_t w2b_set_tally(void* handle, int32_t n, const int32_t* face, const int32_
     H->taxis = axis;
     H->tsign = sign;
     H->ttotal = total;
+    H->version++;
+    return W2B_OK;
+}
+
+int32_t w2b_set_lines(void* handle, int32_t nlines, const int32_t* start, const int32_t* face, const int32_t* axis,
+                      const float* sign, double* q, double* peak, double* time) {
+    if (!handle || nlines < 0 || (nlines && (!start || !face || !axis || !sign || !q || !peak || !time)))
+        return W2B_EINVAL;
+    Handle* H = static_cast<Handle*>(handle);
+    H->nlines = nlines;
+    H->lstart = start;
+    H->lface = face;
+    H->laxis = axis;
+    H->lsign = sign;
+    H->lq = q;
+    H->lpeak = peak;
+    H->ltime = time;
     H->version++;
     return W2B_OK;
 }
@@ -625,6 +657,8 @@ static int advance_runs(Handle* H, const W2BStepper* cfg, const double* t_end, i
     CK(cudaMemcpyAsync(R.max_steps, ms.data(), 8 * n, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(R.refresh_due, rd.data(), 4 * n, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(R.status, st.data(), 4 * n, cudaMemcpyHostToDevice, s));
+    activity_kernel<<<1, 1024, 0, s>>>(make_args(*H), 1);  // the work list of the runs that take a step
+    CKL("advance work list");
     if (H->loop.version != H->version) {
         drop_graphs(*H);
         cudaGraph_t graph;

@@ -22,6 +22,8 @@ constexpr int SLEEP_CHECKS = 2;  // wadi2d/solver/stepper.py:12
 // settings live in the run table (RunTab); a single run is run 0 of a table of one.
 struct Ctl {
     int32_t nact;       // active tiles (all runs)
+    int32_t nwork;      // entries of the work list the face and update passes take
+    int32_t prune;      // a run stopped stepping: the work list is to be rebuilt
     uint32_t any;       // ANY_* bits: OR over the runs of this step's flags
     int32_t nwoken;     // tiles the last rebuild woke
     int32_t status;     // a failure no single run owns (W2B_ETIMEOUT)
@@ -45,6 +47,11 @@ struct RunTab {
     uint32_t* wave_bits;  // max wave speed of the run's tiles, as float bits (waves are never negative)
     int32_t* parity;      // the run's current half of the ping-pong pairs
 };
+
+// Whether run r takes another step (the loop test of wadi2d/solver/stepper.py:106, plus the batch's step limit).
+__device__ __forceinline__ bool live_run(const RunTab& R, int r, const Ctl* ctl) {
+    return ctl->status == 0 && R.status[r] == 0 && R.t[r] < R.t_end[r] - 1e-9 && R.steps_run[r] < R.max_steps[r];
+}
 
 // Layout of a run table of nruns entries in one device block: each array 256-byte aligned.
 __host__ __device__ inline size_t run_table_bytes(int nruns) {
@@ -111,6 +118,8 @@ struct StepArgs {
     int32_t* __restrict__ idle;
     int32_t* __restrict__ is_act;
     int32_t* __restrict__ woken;
+    const int32_t* __restrict__ list;  // the tiles the face and update passes take (ctl->nwork of them)
+    int32_t* __restrict__ work;        // the device loop's work list
     int32_t* __restrict__ scratch;
     float* __restrict__ env[5];
     const uint32_t* __restrict__ bmark;
@@ -126,6 +135,15 @@ struct StepArgs {
     const int32_t* __restrict__ taxis;
     const float* __restrict__ tsign;
     double* __restrict__ ttotal;
+    // design lines: line l's faces are lface[lstart[l] .. lstart[l + 1]); discharge now, its peak |Q| and the time
+    int32_t nlines;
+    const int32_t* __restrict__ lstart;
+    const int32_t* __restrict__ lface;
+    const int32_t* __restrict__ laxis;
+    const float* __restrict__ lsign;
+    double* __restrict__ lq;
+    double* __restrict__ lpeak;
+    double* __restrict__ ltime;
     Ctl* ctl;
     // runs: the run of each tile, and the run table
     const int32_t* __restrict__ tile_run;

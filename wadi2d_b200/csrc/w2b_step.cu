@@ -256,7 +256,7 @@ __global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_co
     __shared__ float rowc[2 * 64 + 1];
     Ctl* ctl = A.ctl;
     if (!(ctl->any & ANY_RUN)) return;
-    const int nact = ctl->nact;
+    const int nwork = ctl->nwork;
     const int tid = threadIdx.x;
     if (tid == 0) {
         mbar_init(&bar, 1);
@@ -278,8 +278,8 @@ __global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_co
                                 A.fl[1], A.fr[1], A.gl[1], A.gr[1], A.ef[1], A.cw[1]};
     uint32_t phase = 0;
     const int lane = tid & 31, warp = tid >> 5;
-    for (int a = blockIdx.x; a < nact; a += gridDim.x) {
-        const int t = A.active[a];
+    for (int a = blockIdx.x; a < nwork; a += gridDim.x) {
+        const int t = A.list[a];
         const int run = A.tile_run[t];
         const int flags = A.R.flags[run];
         if (!(flags & F_RUN)) continue;  // the tile's run has finished: uniform over the CTA
@@ -421,7 +421,7 @@ __global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_con
     __shared__ __align__(8) uint64_t bar;
     Ctl* ctl = A.ctl;
     if (!(ctl->any & ANY_RUN)) return;
-    const int nact = ctl->nact;
+    const int nwork = ctl->nwork;
     const float arrive = ctl->arrive, deep = ctl->deep;
     const int px = A.px;
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
@@ -440,8 +440,8 @@ __global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_con
     const float* SRC = sm + U_OWN + TILE2;
     const float* HC = sm + U_OWN + 2 * TILE2;
     float* rs = sm + U_R;
-    for (int a = blockIdx.x; a < nact; a += gridDim.x) {
-        const int t = A.active[a];
+    for (int a = blockIdx.x; a < nwork; a += gridDim.x) {
+        const int t = A.list[a];
         const int run = A.tile_run[t];
         const int flags = A.R.flags[run];
         if (!(flags & F_RUN)) continue;  // uniform over the CTA
@@ -627,6 +627,30 @@ __global__ void boundary_kernel(StepArgs A, int control) {
         const float qv = A.taxis[m] ? A.q[1][face] : A.q[0][face];
         A.ttotal[m] += R.dt_tally[run] * (double)(A.tsign[m] * qv);
     }
+    // design lines (wadi2d/engine/monitor.py:229-232 at every step): Q = sum of sign q over the line's faces, FP64,
+    // lane-strided then a fixed shuffle tree; the running peak of |Q| and the time at the end of the step
+    const int lane = tid & 31, nwarps = blockDim.x >> 5;
+    for (int l = tid >> 5; l < A.nlines; l += nwarps) {
+        const int s = A.lstart[l], e = A.lstart[l + 1];
+        if (s >= e) continue;
+        const int run = A.tile_run[tile_of_native(A, A.lface[s])];
+        if (!(R.flags[run] & F_RUN)) continue;
+        double acc = 0.0;
+        for (int m = s + lane; m < e; m += 32) {
+            const int f = A.lface[m];
+            acc += (double)A.lsign[m] * (double)(A.laxis[m] ? A.q[1][f] : A.q[0][f]);
+        }
+        for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+        if (lane == 0) {
+            A.lq[l] = acc;
+            const double a = fabs(acc);
+            if (a > A.lpeak[l]) {
+                A.lpeak[l] = a;
+                A.ltime[l] = R.t[run] + R.dt_step[run];
+            }
+        }
+    }
+    __syncthreads();
     for (int r = tid; r < A.nruns; r += blockDim.x) {
         if (!(R.flags[r] & F_RUN)) continue;
         R.parity[r] ^= 1;
@@ -643,6 +667,7 @@ __global__ void boundary_kernel(StepArgs A, int control) {
                 if (R.dt[r] < ctl->dt_min) R.status[r] = W2B_EDTMIN;
             }
         }
+        if (!live_run(R, r, ctl)) ctl->prune = 1;  // its tiles leave the work list at this step's rebuild
     }
 }
 
@@ -656,7 +681,7 @@ __global__ void prestep_kernel(StepArgs A) {
     __syncthreads();
     uint32_t mine = 0u;
     for (int r = threadIdx.x; r < A.nruns; r += blockDim.x) {
-        if (ctl->status != 0 || R.status[r] != 0 || !(R.t[r] < R.t_end[r] - 1e-9) || R.steps_run[r] >= R.max_steps[r]) {
+        if (!live_run(R, r, ctl)) {
             R.flags[r] = 0;
             continue;
         }
@@ -690,6 +715,7 @@ __global__ void endstep_kernel(StepArgs A) { A.R.parity[0] ^= 1; }
 __global__ void setstep_kernel(StepArgs A, float dtf, int want_wave, int want_wet, int nact) {
     Ctl* ctl = A.ctl;
     ctl->nact = nact;
+    ctl->nwork = nact;
     ctl->any = ANY_RUN | (want_wave ? ANY_WAVE : 0u);
     A.R.dtf[0] = dtf;
     A.R.flags[0] = F_RUN | (want_wave ? F_WAVE : 0) | (want_wet ? F_WET : 0);
@@ -724,54 +750,72 @@ __device__ __forceinline__ int block_scan(int flag, int* warp_sums, int* total) 
 }
 
 // rebuild_active(check=True), wadi2d/solver/stepper.py:56-92, for the runs that rebuild at this step: wet or kept
-// tiles and their
-// eight neighbours are active; a tile sleeps after SLEEP_CHECKS checks in a row that did not want it; tiles that
-// join the list are listed in woken for their wet share to be written.
-__global__ void __launch_bounds__(1024) activity_kernel(StepArgs A) {
+// tiles and their eight neighbours are active; a tile sleeps after SLEEP_CHECKS checks in a row that did not want it;
+// tiles that join the list are listed in woken for their wet share to be written. Then the work list: the active tiles
+// of the runs that take another step, rebuilt whenever the active list or the set of stepping runs changed.
+// only_work = 1: the work list alone, before the first step of the device loop.
+__global__ void __launch_bounds__(1024) activity_kernel(StepArgs A, int only_work) {
     Ctl* ctl = A.ctl;
-    if (!(ctl->any & ANY_ACT)) return;
+    const bool rebuild = !only_work && (ctl->any & ANY_ACT);
+    if (!only_work && !rebuild && !ctl->prune) return;
     const int nt = A.ntiles;
     int* wet_eff = A.scratch;
     int* flags = A.scratch + nt;
-    for (int t = threadIdx.x; t < nt; t += blockDim.x) wet_eff[t] = t != 0 && (A.wet[t] != 0 || A.keep[t] != 0);
-    __syncthreads();
-    for (int t = threadIdx.x; t < nt; t += blockDim.x) {
-        if (t == 0) {
-            flags[0] = 0;
-            continue;
-        }
-        const int cur = A.is_act[t];
-        if (!(A.R.flags[A.tile_run[t]] & F_ACT)) {  // this tile's run does not rebuild at this step
-            flags[t] = cur;
-            continue;
-        }
-        int act = wet_eff[t];
-        for (int n = 0; n < 8; ++n) act |= wet_eff[A.nbr[8 * t + n]];
-        if (act)
-            A.idle[t] = 0;
-        else
-            A.idle[t] += 1;
-        act |= cur && A.idle[t] < SLEEP_CHECKS;
-        flags[t] = act | ((act && !cur) << 1);
-        A.is_act[t] = act;
-    }
-    __syncthreads();
     __shared__ int sums[32];
-    int nact = 0, nwoken = 0;
+    if (rebuild) {
+        for (int t = threadIdx.x; t < nt; t += blockDim.x) wet_eff[t] = t != 0 && (A.wet[t] != 0 || A.keep[t] != 0);
+        __syncthreads();
+        for (int t = threadIdx.x; t < nt; t += blockDim.x) {
+            if (t == 0) {
+                flags[0] = 0;
+                continue;
+            }
+            const int cur = A.is_act[t];
+            if (!(A.R.flags[A.tile_run[t]] & F_ACT)) {  // this tile's run does not rebuild at this step
+                flags[t] = cur;
+                continue;
+            }
+            int act = wet_eff[t];
+            for (int n = 0; n < 8; ++n) act |= wet_eff[A.nbr[8 * t + n]];
+            if (act)
+                A.idle[t] = 0;
+            else
+                A.idle[t] += 1;
+            act |= cur && A.idle[t] < SLEEP_CHECKS;
+            flags[t] = act | ((act && !cur) << 1);
+            A.is_act[t] = act;
+        }
+        __syncthreads();
+        int nact = 0, nwoken = 0;
+        for (int base = 0; base < nt; base += blockDim.x) {
+            const int t = base + threadIdx.x;
+            const int f = t < nt ? flags[t] : 0;
+            int tot_a, tot_w;
+            const int oa = block_scan(f & 1, sums, &tot_a);
+            const int ow = block_scan((f >> 1) & 1, sums, &tot_w);
+            if (f & 1) A.active[nact + oa] = t;
+            if (f & 2) A.woken[nwoken + ow] = t;
+            nact += tot_a;
+            nwoken += tot_w;
+        }
+        if (threadIdx.x == 0) {
+            ctl->nact = nact;
+            ctl->nwoken = nwoken;
+        }
+    }
+    // the work list, in tile order: active tiles whose run takes another step
+    int nwork = 0;
     for (int base = 0; base < nt; base += blockDim.x) {
         const int t = base + threadIdx.x;
-        const int f = t < nt ? flags[t] : 0;
-        int tot_a, tot_w;
-        const int oa = block_scan(f & 1, sums, &tot_a);
-        const int ow = block_scan((f >> 1) & 1, sums, &tot_w);
-        if (f & 1) A.active[nact + oa] = t;
-        if (f & 2) A.woken[nwoken + ow] = t;
-        nact += tot_a;
-        nwoken += tot_w;
+        const int f = t > 0 && t < nt && A.is_act[t] && live_run(A.R, A.tile_run[t], ctl);
+        int tot;
+        const int o = block_scan(f, sums, &tot);
+        if (f) A.work[nwork + o] = t;
+        nwork += tot;
     }
     if (threadIdx.x == 0) {
-        ctl->nact = nact;
-        ctl->nwoken = nwoken;
+        ctl->nwork = nwork;
+        ctl->prune = 0;
     }
 }
 

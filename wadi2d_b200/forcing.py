@@ -169,7 +169,7 @@ class Injection:
         self.flows = np.asarray(self.flows, np.float64)
         if np.any(np.diff(self.times) <= 0.0):
             raise ValueError(f"inflow {self.name}: table times must increase")
-        seg = 0.5 * (self.flows[1:] + self.flows[:-1]) * np.diff(self.times)
+        seg = np.diff(self.times) * (self.flows[1:] + self.flows[:-1]) / 2.0  # the trapezoid sum in scipy's order
         self.volume = np.concatenate(([0.0], np.cumsum(seg)))
 
     def volume_at(self, t: float) -> float:

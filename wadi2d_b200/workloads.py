@@ -235,3 +235,103 @@ def ensemble(nruns: int = 64, seed: int = 11, side_min: int = 256, side_max: int
         arf = float(np.round(rng.uniform(0.6, 1.0), 3))
         out.append(EnsembleRun(side, dx, 1000 + r, 0.03 * side * dx, depth, dur, arf))
     return out
+
+
+@dataclass
+class CrestValley:
+    """Configuration 2's inputs on a padded grid: DEM pixels, crest faces, Manning per cell, the lumped inflows, the
+    reservoir and the downstream outfall."""
+
+    n: int
+    dx: float
+    k: int
+    z: np.ndarray
+    crest: object
+    """tables.CrestFaces of the breaklines."""
+    manning: np.ndarray
+    """(ny, nx) Manning n per cell."""
+    inflows: list
+    """Per inflow: (rows, columns) of its cells, the position of the lowest, hydrograph times (s) and flows (m3/s)."""
+    reservoir: tuple
+    """(rows, columns) of the reservoir's cells and its start level (m)."""
+    outfall: tuple
+    """(rows, columns) of the free-outfall cells: the south edge."""
+    t_end: float
+
+
+def crest_valley(n: int = 1024, dx: float = 10.0, k: int = 10, seed: int = 21, relief: float = 120.0,
+                 breaklines: int = 40, t_end: float = 6 * 3600.0) -> CrestValley:  # fmt: skip
+    """Configuration 2: an n x n fractal valley (Hurst 0.75, ``relief`` m) falling south, carved by 3 seeded
+    meandering channels; ``breaklines`` seeded straight breaklines (100-600 m) whose faces carry a crest 0.5-3 m above
+    the higher bed beside them; 3 lumped inflows at the channel heads on the north edge (triangular hydrographs, peaks
+    50-400 m3/s, times to peak 1-3 h, bases 2.67 times that); a 200 x 50 m reservoir on a channel started 4 m above
+    its downstream bed; Manning from seeded Voronoi patches of 0.03-0.06; a free outfall on the south edge."""
+    from wadi2d_b200.tables import CrestFaces
+
+    rng = np.random.default_rng(seed)
+    pad = 32 * int(np.ceil((n + 2) / 32))
+    p = dx / k
+    npx = pad * k
+    L = n * dx
+    c = (np.arange(npx) + 0.5) * p - dx
+    X, Y = np.meshgrid(c, c)  # Y grows south
+    z = relief * (0.6 * (1.0 - Y / L) + 0.4 * (np.abs(X - 0.5 * L) / L) ** 1.5)
+    noise = fractal_noise((npx, npx), 0.75, 1.0, seed)
+    z = z + 0.25 * relief * noise / max(float(np.abs(noise).max()), 1e-9)
+    # three meandering channels from the north edge to the south edge
+    heads = []
+    for m in range(3):
+        x0 = L * (0.2 + 0.3 * m + rng.uniform(-0.05, 0.05))
+        amp, lam, phase = rng.uniform(0.02, 0.06) * L, rng.uniform(0.25, 0.5) * L, rng.uniform(0.0, 2 * np.pi)
+        xc = x0 + amp * np.sin(2 * np.pi * Y / lam + phase)
+        dist = np.abs(X - xc)
+        z = z - np.where(dist < 15.0, 3.0 * (1.0 - dist / 15.0) + 2.0, 2.0 * np.clip(1.0 - (dist - 15.0) / 40.0, 0, 1))
+        heads.append(int(np.clip((x0 + amp * np.sin(phase)) // dx + 1, 2, n - 1)))
+    zc = z.reshape(pad, k, pad, k)
+    cmax = zc.max(axis=(1, 3))
+    cmin = zc.min(axis=(1, 3))
+    crest = CrestFaces.empty((pad, pad))
+    for _ in range(breaklines):
+        j0, i0 = rng.integers(2, n - 1), rng.integers(2, n - 1)
+        length = rng.uniform(100.0, 600.0) / dx
+        ang = rng.uniform(0.0, np.pi)
+        j1 = int(np.clip(j0 + length * np.sin(ang), 2, n - 1))
+        i1 = int(np.clip(i0 + length * np.cos(ang), 2, n - 1))
+        rise = rng.uniform(0.5, 3.0)
+        steps = max(abs(j1 - j0), abs(i1 - i0), 1)
+        jj = np.round(np.linspace(j0, j1, 2 * steps + 1)).astype(int)
+        ii = np.round(np.linspace(i0, i1, 2 * steps + 1)).astype(int)
+        for a in range(jj.size - 1):
+            ja, ia, jb, ib = jj[a], ii[a], jj[a + 1], ii[a + 1]
+            if ib != ia:  # an east-west move crosses the west face of the eastern cell (row ja)
+                je, ie = ja, max(ia, ib)
+                crest.xz[je, ie] = max(cmax[je, ie], cmax[je, ie - 1]) + rise
+            if jb != ja:  # a north-south move crosses the north face of the southern cell (column ib)
+                js, is_ = max(ja, jb), ib
+                crest.yz[js, is_] = max(cmax[js, is_], cmax[js - 1, is_]) + rise
+    # Manning: Voronoi patches
+    seeds = rng.uniform(0, pad, (64, 2))
+    vals = rng.choice([0.03, 0.04, 0.05, 0.06], 64)
+    jg, ig = np.meshgrid(np.arange(pad), np.arange(pad), indexing="ij")
+    best = np.full((pad, pad), np.inf)
+    manning = np.zeros((pad, pad))
+    for s, v in zip(seeds, vals, strict=True):
+        d2 = (jg - s[0]) ** 2 + (ig - s[1]) ** 2
+        closer = d2 < best
+        best[closer] = d2[closer]
+        manning[closer] = v
+    inflows = []
+    for h in heads:
+        peak, tp = rng.uniform(50.0, 400.0), rng.uniform(1.0, 3.0) * 3600.0
+        rows = np.array([1, 1, 1, 2, 2, 2])
+        cols = np.array([h - 1, h, h + 1, h - 1, h, h + 1])
+        low = int(np.argmin(cmin[rows, cols]))
+        inflows.append((rows, cols, low, np.array([0.0, tp, 2.67 * tp]), np.array([0.0, peak, 0.0])))
+    # the reservoir: 20 x 5 cells (200 x 50 m at 10 m) across the middle channel, half-way down
+    h = heads[1]
+    jr = 1 + n // 2
+    rr, cc = np.meshgrid(np.arange(jr - 2, jr + 3), np.arange(h - 10, h + 10), indexing="ij")
+    level = float(cmin[jr + 2, h - 10 : h + 10].min()) + 4.0
+    rows = np.arange(1, 1 + n)
+    return CrestValley(n, dx, k, z, crest, manning, inflows, (rr.ravel(), cc.ravel(), level),
+                       (np.full(n, n), rows), t_end)  # fmt: skip

@@ -300,6 +300,12 @@ int32_t w2b_build_tables_noalloc(const W2BTableIn* in, const W2BTableOut* out, v
 /* Batches (W2BGridDesc.nruns > 1): each run's cell size (host array of nruns), before its first advance. */
 int32_t w2b_set_run_dx(void* handle, const float* dx, int32_t n);
 
+/* The step limiter's reading (wadi2d/solver/limiter.py:31-55 and :163-191: the CPU twin's face_step over one tile):
+ * the wave speed and the new velocity of every own face of `tile` for a step `dt` from the current state, exactly as
+ * the face pass would compute them, into out (device, 4096 floats: wave of the west faces, wave of the north faces,
+ * new u, new v; each 32 x 32, row-major in the tile). Writes nothing else: the state is left as it was. */
+int32_t w2b_face_waves(void* handle, int32_t tile, float dt, float* out, void* stream);
+
 /* Each run's current half of the ping-pong pairs (h, u, v, mx, my): out[r] in {0, 1}, host array of nruns. In a
  * batch the runs' halves differ once their step counts do; w2b_field_ptr, w2b_get_field and w2b_set_field address
  * run 0's half. */

@@ -99,6 +99,7 @@ _SIGNATURES = {
     "w2b_run_table_bytes": [c_i32],
     "w2b_set_run_dx": [c_vp, c_vp, c_i32],
     "w2b_run_halves": [c_vp, c_vp, c_vp],
+    "w2b_face_waves": [c_vp, c_i32, c_f32, c_vp, c_vp],
     "w2b_source_runs": [c_vp, c_i64, c_vp, c_vp, c_vp],
     "w2b_set_lines": [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
     "w2b_advance_runs": [c_vp, ctypes.POINTER(Stepper), c_vp, c_i64, c_vp, c_vp],

@@ -14,6 +14,7 @@
 
 namespace w2b {
 cudaError_t faces_setup();
+void launch_probe(const StepArgs& A, int t, float dt, float* out, cudaStream_t s);
 void launch_cbrt_check(uint32_t first, uint32_t count, unsigned long long* out, cudaStream_t s);
 int faces_occupancy();
 void launch_faces(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s);
@@ -730,6 +731,15 @@ int32_t w2b_advance_runs(void* handle, const W2BStepper* cfg, const double* t_en
     if (!handle || !cfg || !clocks || !t_end || max_steps < 0 || cfg->dt_every < 1 || cfg->active_every < 1)
         return W2B_EINVAL;
     return advance_runs(static_cast<Handle*>(handle), cfg, t_end, max_steps, clocks, (cudaStream_t)stream);
+}
+
+int32_t w2b_face_waves(void* handle, int32_t tile, float dt, float* out, void* stream) {
+    if (!handle || !out || !(dt > 0.0f)) return W2B_EINVAL;
+    Handle* H = static_cast<Handle*>(handle);
+    if (tile < 1 || tile >= H->g.ntiles) return W2B_EINVAL;
+    launch_probe(make_args(*H), tile, dt, out, (cudaStream_t)stream);
+    CKL("w2b_face_waves");
+    return W2B_OK;
 }
 
 int32_t w2b_run_halves(void* handle, int32_t* out, void* stream) {

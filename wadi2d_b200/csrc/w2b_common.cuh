@@ -172,13 +172,10 @@ __device__ __forceinline__ bool cube_above(double m, float x) {
     return (double)x - p > e;
 }
 
-// The float nearest the cube root of x. Numba's float32 cbrt is float(cbrt(double(x))), the cube root rounded
-// once to double and once to float; this returns the correctly rounded float, which is the same number whenever
-// the double root is within the distance of cbrt(x) from the nearest float midpoint (w2b_selftest_cbrt compares the
-// two over every positive float). Method: cbrtf gives a float within one ulp; of it and its two neighbours the
-// answer is decided by comparing x with the cubes of the two midpoints (cube_above). No midpoint's cube is a float
-// (a 25-bit odd significand cubes to more than 72 bits), so the comparison never ties.
-__device__ __forceinline__ float cbrt32(float x) {
+// The float nearest the cube root of x, decided exactly in double: cbrtf gives a float within one ulp; of it and its
+// two neighbours the answer is decided by comparing x with the cubes of the two midpoints (cube_above). The path for
+// the ends of the float range, and for the rare inputs whose FP32 decision in cbrt32 is too close to call.
+static __device__ __noinline__ float cbrt32_exact(float x) {
     if (!(x > 0.0f) || x > 3.0e38f) return (float)cbrt((double)x);  // zero, negative, NaN, huge: the double path
     const float y = cbrtf(x);
     const float yu = __int_as_float(__float_as_int(y) + 1);
@@ -186,6 +183,56 @@ __device__ __forceinline__ float cbrt32(float x) {
     if (cube_above(0.5 * ((double)y + (double)yu), x)) return yu;
     if (!cube_above(0.5 * ((double)yd + (double)y), x)) return yd;
     return y;
+}
+
+// The hardware's base-2 logarithm, exponential and reciprocal estimates (PTX lg2.approx, ex2.approx, rcp.approx; the
+// inputs here are positive normal floats).
+__device__ __forceinline__ float lg2_approx(float x) {
+    float y;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float ex2_approx(float x) {
+    float y;
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+// The float nearest the cube root of x. Numba's float32 cbrt is float(cbrt(double(x))), the cube root rounded once to
+// double and once to float; this returns the correctly rounded float, which is the same number whenever the double
+// root is within the distance of cbrt(x) from the nearest float midpoint (w2b_selftest_cbrt compares the two over
+// every positive float). Method, in FP32 for 2^-96 <= x <= 2^96:
+//  - y0 = 2^(log2(x) / 3) from the hardware estimates is within 2^-19 of the root t; one Newton step,
+//    y = y0 - (y0^3 - x) / (3 y0^2), with y0^3 - x formed from an error-free square, is within half an ulp plus
+//    2^-36 t of t, so the answer is y or its neighbour on the side of t;
+//  - d = x - y^3 to within 2^-45 x: y^2 = q + qe and q y = c + ce exactly (FMA error-free products), x - c exactly
+//    (Sterbenz), the tail qe y rounded once; its sign gives the side of t;
+//  - with s the signed half-ulp step to that side's midpoint m = y + s, x - m^3 = d - (3 y^2 s + 3 y s^2 + s^3), the
+//    roundings below 2^-44 x in all; a value beyond 2^-42 x has a certain sign and picks the answer, a value inside
+//    it (about one input in 2^17) and x outside the range go to cbrt32_exact.
+__device__ __forceinline__ float cbrt32(float x) {
+    if (!(x >= 0x1p-96f && x <= 0x1p96f)) return cbrt32_exact(x);
+    const float y0 = ex2_approx(lg2_approx(x) * 0.333333343f);
+    const float p = y0 * y0;
+    const float pe = fmaf(y0, y0, -p);
+    const float r = fmaf(p, y0, -x) + pe * y0;  // y0^3 - x
+    const float y = fmaf(-r, rcp_approx(3.0f * p), y0);
+    const float q = y * y;
+    const float qe = fmaf(y, y, -q);
+    const float c = q * y;
+    const float ce = fmaf(q, y, -c);
+    const float d = ((x - c) - ce) - qe * y;  // x - y^3
+    const int bits = __float_as_int(y);
+    const float nb = __int_as_float(d >= 0.0f ? bits + 1 : bits - 1);
+    const float st = 0.5f * (nb - y);  // exact: half the gap to the neighbour, signed
+    const float z = d - (3.0f * q * st + 3.0f * y * st * st);
+    if (fabsf(z) <= x * 0x1p-42f) return cbrt32_exact(x);
+    return (z > 0.0f) == (d >= 0.0f) ? nb : y;
 }
 // Python max/min on two ordered floats (the first argument wins a tie).
 __device__ __forceinline__ float fmax32(float a, float b) { return a >= b ? a : b; }

@@ -77,16 +77,22 @@ __device__ __forceinline__ void face_a(const float* sm, int b, int local, const 
 
 // Parts B and C: the momentum terms (faces.cu:50-100, table-free), then the lookup, section, friction, crest cap,
 // outputs and wave speed (faces.cu:43-44, :52-63, :102-145). Returns the wave speed.
-template <int AX>
+// PROBE: write the face's new velocity to probe_un[local] and nothing of the state (the step-limiter probe).
+template <int AX, bool PROBE = false>
 __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int k, const StepArgs& A, int t,
-                                         const FaceA& F, float dt, float dx, int want_wave, const float* rowc, int p) {
+                                         const FaceA& F, float dt, float dx, int want_wave, const float* rowc, int p,
+                                         float* probe_un = nullptr) {
     constexpr int S = AX == 0 ? 1 : BOXW;
     constexpr int PP = AX == 0 ? BOXW : 1;
     const W2BParams& P = A.P;
     if (!F.live) {
-        A.uu[AX][1 - p][k] = 0.0f;
-        A.mm[AX][1 - p][k] = 0.0f;
-        A.q1[AX][k] = 0.0f;
+        if constexpr (PROBE) {
+            probe_un[local] = 0.0f;
+        } else {
+            A.uu[AX][1 - p][k] = 0.0f;
+            A.mm[AX][1 - p][k] = 0.0f;
+            A.q1[AX][k] = 0.0f;
+        }
         return 0.0f;
     }
     const float ZERO = 0.0f, HALF = 0.5f, ONE = 1.0f;
@@ -207,9 +213,13 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
             un = qn / fmax32(area * rho, 1e-12f);
         }
     }
-    A.uu[AX][1 - p][k] = un;
-    A.mm[AX][1 - p][k] = abar * un;
-    A.q1[AX][k] = qn;
+    if constexpr (PROBE) {
+        probe_un[local] = un;
+    } else {
+        A.uu[AX][1 - p][k] = un;
+        A.mm[AX][1 - p][k] = abar * un;
+        A.q1[AX][k] = qn;
+    }
     if (!want_wave) return ZERO;
     if (not_finite(un)) return 1e30f;
     const float* D = sm + F_D * BOX;
@@ -361,7 +371,62 @@ void launch_cbrt_check(uint32_t first, uint32_t count, unsigned long long* out, 
     cbrt_check_kernel<<<148 * 16, 256, 0, s>>>(first, count, out);
 }
 
+// The wave speed and the new velocity of every own face of tile t for a step dt from the current state, as the face
+// pass would compute them, written to out ([wx | wy | un_x | un_y], 1024 each, tile layout) and nothing else: the
+// device side of the step limiter (wadi2d/solver/limiter.py:31-55, the CPU twin's face_step on one tile). One CTA;
+// the tile's image is filled with plain loads (the boxes lie inside the guard ring of the NATIVE arrays).
+__global__ void __launch_bounds__(1024) probe_kernel(StepArgs A, int t, float dt, float* __restrict__ out) {
+    extern __shared__ __align__(128) float sm[];
+    __shared__ float rowc[2 * 64 + 1];
+    const int tid = threadIdx.x;
+    const int run = A.tile_run[t];
+    const int p = A.R.parity[run];
+    const float dx = A.R.dx[run];
+    const int tj = A.tiles[2 * t], ti = A.tiles[2 * t + 1];
+    const int x0 = ti * TILE + GX - 4, y0 = tj * TILE + GY - 2;
+    const float* boxes[NBOX] = {A.d, A.hh[p], A.uu[0][p], A.uu[1][p], A.q[0], A.q[1], A.om, A.zc[0], A.zc[1]};
+    for (int idx = tid; idx < BOX; idx += blockDim.x) {
+        const size_t k = (size_t)(y0 + idx / BOXW) * A.px + x0 + idx % BOXW;
+        for (int f = 0; f < NBOX; ++f) sm[f * BOX + idx] = boxes[f][k];
+    }
+    const float* statics[12] = {A.fl[0], A.fr[0], A.gl[0], A.gr[0], A.ef[0], A.cw[0],
+                                A.fl[1], A.fr[1], A.gl[1], A.gr[1], A.ef[1], A.cw[1]};
+    for (int idx = tid; idx < TILE2; idx += blockDim.x) {
+        const size_t k = (size_t)(tj * TILE + GY + idx / TILE) * A.px + ti * TILE + GX + idx % TILE;
+        sm[SM_M + idx] = A.mm[0][p][k];
+        sm[SM_M + TILE2 + idx] = A.mm[1][p][k];
+        for (int f = 0; f < 12; ++f) sm[SM_ST + f * TILE2 + idx] = statics[f][(size_t)t * TILE2 + idx];
+    }
+    if (tid < A.rows - 1) {
+        const float m = (float)(A.rows - 1);
+        const float c0 = (float)tid / m;
+        const float c1 = (float)(tid + 1) / m;
+        rowc[2 * tid] = c0 * c0;
+        rowc[2 * tid + 1] = c1 * c1 - c0 * c0;
+    } else if (tid == A.rows - 1) {
+        const float m = (float)(A.rows - 1);
+        const float c = (m - 1.0f) / m;
+        rowc[2 * tid] = 1.0f - c * c;
+    }
+    __syncthreads();
+    const int jj = tid >> 5, ii = tid & 31;
+    const int local = jj * TILE + ii;
+    const int b = (jj + 2) * BOXW + ii + 4;
+    const int k = (tj * TILE + GY + jj) * A.px + ti * TILE + GX + ii;
+    FaceA fx, fy;
+    face_a<0>(sm, b, local, A, t, fx);
+    face_a<1>(sm, b, local, A, t, fy);
+    out[local] = face_bc<0, true>(sm, b, local, k, A, t, fx, dt, dx, 1, rowc, p, out + 2 * TILE2);
+    out[TILE2 + local] = face_bc<1, true>(sm, b, local, k, A, t, fy, dt, dx, 1, rowc, p, out + 3 * TILE2);
+}
+
+void launch_probe(const StepArgs& A, int t, float dt, float* out, cudaStream_t s) {
+    probe_kernel<<<1, 1024, SM_FLOATS * 4, s>>>(A, t, dt, out);
+}
+
 cudaError_t faces_setup() {
+    const cudaError_t e = cudaFuncSetAttribute(probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SM_FLOATS * 4);
+    if (e != cudaSuccess) return e;
     return cudaFuncSetAttribute(faces_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, FACES_SMEM);
 }
 

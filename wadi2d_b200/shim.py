@@ -2,8 +2,10 @@
 
 ``install()`` wraps ``wadi2d.solver.model.select_backend`` (which ``Model`` imported by name from
 wadi2d/solver/backend.py:58-75) so that ``"b200"``, and ``"auto"``/``"gpu"`` when a CUDA device is present, return a
-``B200Backend``; and it replaces ``wadi2d.engine.monitor.Maxima`` and ``Tally`` (wadi2d/engine/maxima.py:103-192) with
-this package's device versions when the model's backend is a B200 one. ``uninstall()`` restores the originals.
+``B200Backend``; it replaces ``wadi2d.engine.monitor.Maxima`` and ``Tally`` (wadi2d/engine/maxima.py:103-192) with
+this package's device versions when the model's backend is a B200 one; and it routes the run monitor's step-limiter
+reading (``step_limiter`` as wadi2d/engine/step_limiter.py:15 imported it) to ``wadi2d_b200.limiter`` for B200
+models. ``uninstall()`` restores the originals.
 """
 
 from __future__ import annotations
@@ -58,6 +60,22 @@ def install(auto: bool = True) -> None:
             return factory
 
         setattr(monitor, name, make())
+    try:
+        logmod = importlib.import_module("wadi2d.engine.step_limiter")
+    except Exception:  # the limiter log's optional dependencies may be absent
+        return
+    if "step_limiter" not in _saved:
+        _saved["step_limiter"] = logmod.step_limiter
+    theirs = _saved["step_limiter"]
+
+    def step_limiter(model_, tables=None):
+        if isinstance(getattr(model_, "backend", None), B200Backend):
+            from wadi2d_b200.limiter import step_limiter as mine
+
+            return mine(model_, tables)
+        return theirs(model_, tables)
+
+    logmod.step_limiter = step_limiter
 
 
 def uninstall() -> None:
@@ -70,3 +88,9 @@ def uninstall() -> None:
     for name in ("Maxima", "Tally"):
         if name in _saved:
             setattr(monitor, name, _saved.pop(name))
+    try:
+        logmod = importlib.import_module("wadi2d.engine.step_limiter")
+    except Exception:
+        return
+    if "step_limiter" in _saved:
+        logmod.step_limiter = _saved.pop("step_limiter")

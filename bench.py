@@ -57,6 +57,7 @@ def parse():
     p.add_argument("--e2e-windows", type=int, default=4)
     p.add_argument("--full-run", action="store_true",
                    help="the whole 36 h run of configuration 3 from dry ground, with its mass balance")
+    p.add_argument("--sim-hours", type=float, default=36.0, help="--full-run: simulated hours (configuration 3: 36)")
     p.add_argument("--ensemble", action="store_true",
                    help="configuration 4: the storm sweep as one batch against the same runs one after another")
     p.add_argument("--runs", type=int, default=64, help="runs of the ensemble")
@@ -256,13 +257,14 @@ def full_run(args) -> None:
     setup = time.perf_counter() - t0
     torch.cuda.synchronize(dev)
     w0 = time.perf_counter()
-    out = run_windows(m, c.t_end, rain=rain, window=30.0, maxima=maxima, tally=tally, storage=storage)
+    t_end = min(c.t_end, args.sim_hours * 3600.0)
+    out = run_windows(m, t_end, rain=rain, window=30.0, maxima=maxima, tally=tally, storage=storage)
     torch.cuda.synchronize(dev)
     wall = time.perf_counter() - w0
     b = out.balance
     env = maxima.fields()
     line = {
-        "run": "configuration 3, 36 h", "cells": args.n * args.n, "steps": out.steps, "windows": out.windows,
+        "run": f"configuration 3, {t_end / 3600.0:g} h", "cells": args.n * args.n, "steps": out.steps, "windows": out.windows,
         "wall_s": wall, "setup_s": setup, "runs_per_h": 3600.0 / (wall + setup),
         "cell_steps_per_s": args.n * args.n * out.steps / wall,
         "rain_m3": b.rain, "outflow_m3": b.outflow, "storage_m3": b.storage, "mass_error": b.relative,

@@ -19,13 +19,18 @@ import numpy as np
 from wadi2d_b200 import _lib
 from wadi2d_b200.backend import B200Backend, BoundaryCells, NumericsRecord
 from wadi2d_b200.config import Numerics
-from wadi2d_b200.forcing import Balance
+from wadi2d_b200.forcing import Balance, UniformStorm
 from wadi2d_b200.grid import TileGrid
 from wadi2d_b200.layout import GX, GY, STRIDE2, TILE, TILE2, native_of_ref
 from wadi2d_b200.maxima import NAMES, NOT_ARRIVED
 from wadi2d_b200.state import level_field, plan_field, state_index, to_state
 from wadi2d_b200.stepper import NumericalFailure, Stepper
 from wadi2d_b200.tablebuild import TILE_FIELDS, DeviceGridTables
+
+
+CLOCK = np.dtype([("t", "f8"), ("dt", "f8"), ("nsteps", "i8"), ("refresh_due", "i4"), ("status", "i4"),
+                  ("wave_max", "f4"), ("nact", "i4")])
+"""W2BClock as a numpy record (the same fields, offsets and 40-byte size), so that a batch's clocks pass as one array."""
 
 
 @dataclass
@@ -154,6 +159,10 @@ class Batch:
         self.status = np.zeros(n, np.int32)
         self.boundary_tiles = np.zeros(0, np.int64)
         self._source_tiles = np.zeros(nt, bool)
+        # the device holds the activity state between advances: the host's copies are pulled before a host rebuild,
+        # and its keep flags and idle counters pushed only when the host changed them
+        self._device_newer = False
+        self._push_keep = self._push_idle = True
         self._tally = None
         self._tally_slices: list[slice] = [slice(0, 0)] * n
 
@@ -232,6 +241,15 @@ class Batch:
 
     # ------------------------------------------------------------------ the reference model's setters, per run
 
+    def _pull(self) -> None:
+        """The device's active list and idle counters into the host's copies, before a host rebuild."""
+        if not self._device_newer:
+            return
+        b = self.backend
+        b.active_tiles = b._t["active"][: b.nact].cpu().numpy().astype(np.int32)
+        self.stepper.idle[:] = b._t["idle"].cpu().numpy()
+        self._device_newer = False
+
     def set_depth(self, hbars: list) -> None:
         """Mean depth grids (one per run; None: dry), levels through each run's tables in FP64, zero velocities."""
         self._same_halves("set_depth")
@@ -251,7 +269,9 @@ class Batch:
         wet = np.zeros(grid.ntiles, np.int32)
         wet[1:] = blocks[grid.tiles[1:, 0], grid.tiles[1:, 1]]
         b.wet[:] = wet
+        self._pull()
         self.stepper.rebuild_active()
+        self._push_idle = True
 
     def set_source(self, rates: list) -> None:
         """Net source rate grids, m/s (one per run; None: no source). Tiles with a source stay active."""
@@ -273,6 +293,8 @@ class Batch:
         self.refresh_due[:] = 1
 
     def _keep(self) -> None:
+        self._pull()
+        self._push_keep = True
         st = self.stepper
         st.keep_active[:] = self._source_tiles
         st.keep_active[self.boundary_tiles] = True
@@ -338,25 +360,25 @@ class Batch:
         te = np.ascontiguousarray(np.broadcast_to(np.asarray(t_end, np.float64), (n,)))
         b, st, num = self.backend, self.stepper, self.num
         torch = self.torch
-        b._t["keep"].copy_(torch.as_tensor(st.keep_active.astype(np.int32), device=b.device))
-        b._t["idle"].copy_(torch.as_tensor(st.idle, device=b.device))
+        if self._push_keep:
+            b._t["keep"].copy_(torch.as_tensor(st.keep_active.astype(np.int32), device=b.device))
+            self._push_keep = False
+        if self._push_idle:
+            b._t["idle"].copy_(torch.as_tensor(st.idle, device=b.device))
+            self._push_idle = False
         cfg = _lib.Stepper(num.cfl, num.wave_floor, num.dt_max, num.dt_min, num.dt_every, num.active_every,
                            int(st.adaptive_active), int(max_every), arrive, deep)  # fmt: skip
-        clocks = (_lib.Clock * n)()
-        for r in range(n):
-            clocks[r] = _lib.Clock(float(self.t[r]), float(self.dt[r]), int(self.nsteps[r]), int(self.refresh_due[r]),
-                                   0, 0.0, int(b.nact))  # fmt: skip
+        clocks = np.zeros(n, CLOCK)
+        clocks["t"], clocks["dt"], clocks["nsteps"] = self.t, self.dt, self.nsteps
+        clocks["refresh_due"], clocks["nact"] = self.refresh_due, b.nact
         limit = (1 << 62) if max_steps is None else int(max_steps)
-        status = int(_lib.lib().w2b_advance_runs(b.handle, ctypes.byref(cfg), te.ctypes.data, limit, clocks,
-                                                 b._stream()))  # fmt: skip
-        for r in range(n):
-            self.t[r], self.dt[r], self.nsteps[r] = clocks[r].t, clocks[r].dt, clocks[r].nsteps
-            self.status[r] = clocks[r].status
+        status = int(_lib.lib().w2b_advance_runs(b.handle, ctypes.byref(cfg), te.ctypes.data, limit,
+                                                 clocks.ctypes.data, b._stream()))  # fmt: skip
+        self.t[:], self.dt[:], self.nsteps[:] = clocks["t"], clocks["dt"], clocks["nsteps"]
+        self.status[:] = clocks["status"]
         self.refresh_due[:] = 0
-        nact = int(clocks[0].nact)
-        b.active_tiles = b._t["active"][:nact].cpu().numpy().astype(np.int32)
-        b.nact = nact
-        st.idle[:] = b._t["idle"].cpu().numpy()
+        b.nact = int(clocks["nact"][0])
+        self._device_newer = True
         if status not in (_lib.OK, _lib.ENONFINITE, _lib.EDTMIN):
             raise _lib.W2BError(status, "w2b_advance_runs")
         if raise_on_failure and np.any(self.status != 0):
@@ -383,6 +405,11 @@ class Batch:
         rates_dev = torch.zeros(n, dtype=torch.float32, device=b.device)
         area = self.dx.astype(np.float64) ** 2
         books = [Balance() for _ in range(n)]
+        uniform = all(isinstance(x, UniformStorm) for x in storms)
+        if uniform:  # every storm linear in time: the cumulative depths of all runs at once, element for element
+            total = np.array([x.total_depth for x in storms], np.float64)
+            dur = np.array([x.duration_minutes for x in storms], np.float64)
+        falling_last = None
         while True:
             live = self.t < te - 1e-9
             if not live.any():
@@ -390,31 +417,41 @@ class Batch:
             t0 = self.t.copy()
             t1 = np.where(live, np.minimum(t0 + window, te), t0)
             rates = np.zeros(n, np.float32)
-            falling = np.zeros(n, bool)
+            if uniform:
+                f0 = total * np.clip((t0 / 60.0) / dur, 0.0, 1.0)
+                f1 = total * np.clip((t1 / 60.0) / dur, 0.0, 1.0)
+            else:
+                f0, f1 = np.zeros(n), np.zeros(n)
+                for r in np.nonzero(live)[0]:
+                    f0[r] = float(np.asarray(storms[r].cumulative_depth(np.array([t0[r] / 60.0])))[0])
+                    f1[r] = float(np.asarray(storms[r].cumulative_depth(np.array([t1[r] / 60.0])))[0])
+            span = np.where(live, t1 - t0, 1.0)
+            rates[live] = ((f1 - f0) / (1000.0 * span))[live].astype(np.float32)
+            falling = live & (f1 > f0)
             for r in np.nonzero(live)[0]:
-                f0 = float(np.asarray(storms[r].cumulative_depth(np.array([t0[r] / 60.0])))[0])
-                f1 = float(np.asarray(storms[r].cumulative_depth(np.array([t1[r] / 60.0])))[0])
-                rates[r] = np.float32((f1 - f0) / (1000.0 * (t1[r] - t0[r])))
-                falling[r] = f1 > f0
                 books[r].rain += float(rates[r]) * counts[r] * area[r] * (t1[r] - t0[r])
             rates_dev.copy_(torch.as_tensor(rates))
             _lib.call("w2b_source_runs", b.handle, int(cat.numel()), cat.data_ptr(), rates_dev.data_ptr(),
                       b._stream())  # fmt: skip
-            if self.stepper.adaptive_active:
+            if self.stepper.adaptive_active and (falling_last is None
+                                                 or not np.array_equal(falling & live, falling_last)):
                 keep = [run_tiles[r] for r in np.nonzero(falling & live)[0]]
                 tiles = np.concatenate(keep) if keep else np.zeros(0, np.int64)
                 st = self.stepper
                 if np.all(st.keep_active[tiles]):
                     # no tile joins the kept set: the host's rebuild (retain) would leave the active list as it is,
                     # since every device rebuild already took the wet and kept tiles with their neighbours; only the
-                    # kept flags change (they go to the device with the next advance)
-                    self._source_tiles[:] = False
-                    self._source_tiles[tiles] = True
-                    st.keep_active[:] = self._source_tiles
-                    st.keep_active[self.boundary_tiles] = True
-                    st.keep_active[0] = False
+                    # kept flags change (they go to the device with the next advance, when they do change)
+                    if falling_last is None or not np.array_equal(falling & live, falling_last):
+                        self._source_tiles[:] = False
+                        self._source_tiles[tiles] = True
+                        st.keep_active[:] = self._source_tiles
+                        st.keep_active[self.boundary_tiles] = True
+                        st.keep_active[0] = False
+                        self._push_keep = True
                 else:
                     self.set_source_tiles(tiles)
+                falling_last = falling & live
             self.refresh_due[live] = 1
             self.advance(t1, max_every=max_every, arrive=arrive, deep=deep)
         out = self.tally_volumes()

@@ -317,6 +317,31 @@ int32_t w2b_run_halves(void* handle, int32_t* out, void* stream);
 int32_t w2b_advance_runs(void* handle, const W2BStepper* cfg, const double* t_end, int64_t max_steps,
                          W2BClock* clocks, void* stream);
 
+/* ---- the surrogate's network (no counterpart in the reference: the storm-sweep surrogate of the critical-duration
+ * search). BF16 operands are 16-bit bfloat16 arrays; every pointer is device memory. ---- */
+
+/* c (m x n, FP32, row-major) = a (m x k, BF16, row-major) b^T (b: n x k, BF16, row-major) + bias (n, FP32, or NULL),
+ * on the tensor cores (tcgen05.mma, FP32 accumulator in tensor memory). 16 <= n <= 256, n % 16 == 0, k % 16 == 0,
+ * a and b 16-byte aligned. status (device int32) is set to W2B_ETIMEOUT if a bounded wait gave up. */
+int32_t w2b_mma_gemm(const void* a, const void* b, int32_t m, int32_t n, int32_t k, const float* bias, float* c,
+                     int32_t* status, void* stream);
+/* out (BF16) = relu(z) (relu = 1) or z, n elements. */
+int32_t w2b_bf16_act(const float* z, int64_t n, int32_t relu, void* out, void* stream);
+/* dz (BF16) = g where z > 0, else 0. */
+int32_t w2b_relu_back(const float* g, const float* z, int64_t n, void* dz, void* stream);
+/* xt (cols x rows_pad, BF16) = x^T (x: rows x cols, BF16), columns past rows zero. */
+int32_t w2b_transpose_bf16(const void* x, int32_t rows, int32_t cols, int32_t rows_pad, void* xt, void* stream);
+/* dy (m_pad x n, BF16) = scale (y - t) on the first m rows, 0 on the rest; partial[64] (FP64) = the blocks' sums of
+ * (y - t)^2. */
+int32_t w2b_mse_grad(const float* y, const float* t, int32_t m, int32_t m_pad, int32_t n, float scale, void* dy,
+                     double* partial, void* stream);
+/* out[c] (FP32) = sum over the rows of x[r][c] (x BF16, rows x cols). */
+int32_t w2b_colsum_bf16(const void* x, int32_t rows, int32_t cols, float* out, void* stream);
+/* One Adam step on n FP32 weights w with gradient g and moments m, v (lr_t: the bias-corrected step size), and wb
+ * (BF16, or NULL) = the new weights. */
+int32_t w2b_adam(float* w, const float* g, float* m, float* v, int64_t n, float lr_t, float b1, float b2, float eps,
+                 void* wb, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

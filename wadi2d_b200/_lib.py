@@ -100,6 +100,13 @@ _SIGNATURES = {
     "w2b_set_run_dx": [c_vp, c_vp, c_i32],
     "w2b_run_halves": [c_vp, c_vp, c_vp],
     "w2b_face_waves": [c_vp, c_i32, c_f32, c_vp, c_vp],
+    "w2b_mma_gemm": [c_vp, c_vp, c_i32, c_i32, c_i32, c_vp, c_vp, c_vp, c_vp],
+    "w2b_bf16_act": [c_vp, c_i64, c_i32, c_vp, c_vp],
+    "w2b_relu_back": [c_vp, c_vp, c_i64, c_vp, c_vp],
+    "w2b_transpose_bf16": [c_vp, c_i32, c_i32, c_i32, c_vp, c_vp],
+    "w2b_mse_grad": [c_vp, c_vp, c_i32, c_i32, c_i32, c_f32, c_vp, c_vp, c_vp],
+    "w2b_colsum_bf16": [c_vp, c_i32, c_i32, c_vp, c_vp],
+    "w2b_adam": [c_vp, c_vp, c_vp, c_vp, c_i64, c_f32, c_f32, c_f32, c_f32, c_vp, c_vp],
     "w2b_source_runs": [c_vp, c_i64, c_vp, c_vp, c_vp],
     "w2b_set_lines": [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
     "w2b_advance_runs": [c_vp, ctypes.POINTER(Stepper), c_vp, c_i64, c_vp, c_vp],

@@ -12,7 +12,7 @@ from pathlib import Path
 
 PKG = Path(__file__).resolve().parent
 ROOT = PKG.parent
-SOURCES = ["w2b_step.cu", "w2b_tables.cu", "w2b_source.cu", "w2b_api.cu"]
+SOURCES = ["w2b_step.cu", "w2b_tables.cu", "w2b_source.cu", "w2b_mlp.cu", "w2b_api.cu"]
 OUT = PKG / "libwadi_b200.so"
 
 NVCC_FLAGS = [

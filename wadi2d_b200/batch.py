@@ -409,6 +409,9 @@ class Batch:
         if uniform:  # every storm linear in time: the cumulative depths of all runs at once, element for element
             total = np.array([x.total_depth for x in storms], np.float64)
             dur = np.array([x.duration_minutes for x in storms], np.float64)
+        kind = type(storms[0])
+        many = getattr(kind, "cumulative_many", None) if all(type(x) is kind for x in storms) else None
+        stacked = kind.stack(storms) if many is not None else None
         falling_last = None
         while True:
             live = self.t < te - 1e-9
@@ -420,6 +423,9 @@ class Batch:
             if uniform:
                 f0 = total * np.clip((t0 / 60.0) / dur, 0.0, 1.0)
                 f1 = total * np.clip((t1 / 60.0) / dur, 0.0, 1.0)
+            elif many is not None:  # storms of one kind that rate many at once, as each would alone
+                f0 = many(stacked, t0 / 60.0)
+                f1 = many(stacked, t1 / 60.0)
             else:
                 f0, f1 = np.zeros(n), np.zeros(n)
                 for r in np.nonzero(live)[0]:

@@ -65,6 +65,11 @@ def parse():
     p.add_argument("--recession-min", type=float, default=30.0, help="simulated time after each storm, minutes")
     p.add_argument("--time-scale", type=float, default=1.0, help="share of each run's simulated time to step")
     p.add_argument("--skip-plain", action="store_true", help="the batch only (no one-after-another sweep)")
+    p.add_argument("--critical", action="store_true",
+                   help="configuration 5: the critical-duration search, screened by the network, against the sweep")
+    p.add_argument("--candidates", type=int, default=400, help="--critical: candidate storms")
+    p.add_argument("--train-runs", type=int, default=96, help="--critical: solver runs the network learns from")
+    p.add_argument("--plain-sample", type=int, default=8, help="--critical: runs timed one after another")
     return p.parse_args()
 
 
@@ -416,6 +421,107 @@ def ensemble_run(args) -> None:
         dist.destroy_process_group()
 
 
+def critical_run(args) -> None:
+    """Configuration 5 at args.n cells (256 by default; the configuration names 1024): which of args.candidates storms
+    (0.5-48 h log-uniform, 20-200 mm, ARF 0.6-1.0, patterns a seeded convex mix of 4 alternating-block hyetographs)
+    gives the largest peak flow at the main design point. Three ways, timed with CUDA events: every candidate through
+    the solver as batches (the exhaustive sweep), the network's screen (solver runs of args.train_runs candidates,
+    training, ranking, solver runs of the top 5 %), and one solver run after another on a sample of args.plain_sample
+    candidates, whose time per simulated hour gives the one-after-another sweep's runs/h. A non-learned screen (the
+    same share ranked by peak block intensity) shows what the network adds."""
+    import torch
+
+    from wadi2d_b200 import critical as C
+    from wadi2d_b200.config import Numerics
+    from wadi2d_b200.maxima import Lines, Tally
+    from wadi2d_b200.model import Model
+    from wadi2d_b200.run import DeviceRain, run_windows
+
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+
+    def timed(fn):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        out = fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return out, e0.elapsed_time(e1) / 1e3
+
+    n = args.n if args.n != 4096 else 256
+    t0 = time.perf_counter()
+    cat = C.prepare(n=n, dx=10.0, k=4, seed=17, device=dev)
+    setup = time.perf_counter() - t0
+    storms = C.candidates(args.candidates, seed=5)
+    x = C.features(storms)
+    rec = 1.0
+    sim_h = np.array([s.duration_h + rec for s in storms])
+    full, full_s = timed(lambda: C.solve(cat, storms, recession_h=rec))
+    point = 0
+    crit = int(np.argmax(full["peak_q"][:, point]))
+    rng = np.random.default_rng(11)
+    train = rng.choice(len(storms), size=args.train_runs, replace=False)
+    res_tr, tr_s = timed(lambda: C.solve(cat, [storms[i] for i in train], recession_h=rec))
+    y_tr = C.targets(res_tr)
+    (order, pred, losses), fit_s = timed(lambda: C.screen(x[train], y_tr, x, top=0.05, point=point, iters=3000))
+    rerun = [int(i) for i in order if i not in set(train.tolist())]
+    res_rr, rr_s = timed(lambda: C.solve(cat, [storms[i] for i in rerun], recession_h=rec) if rerun else None)
+    solved = {int(i): float(res_tr["peak_q"][k, point]) for k, i in enumerate(train)}
+    for k, i in enumerate(rerun):
+        solved[i] = float(res_rr["peak_q"][k, point])
+    found = max(solved, key=solved.get)
+    screen_s = tr_s + fit_s + rr_s
+    # the same share ranked without the network: by the storm's peak block intensity (descriptor 9)
+    k = len(order)
+    naive = set(np.argsort(x[:, 9])[::-1][:k].tolist()) | set(train.tolist())
+    naive_found = max(naive, key=lambda i: full["peak_q"][i, point])
+    held = np.setdiff1d(np.arange(len(storms)), train)
+    truth = np.log1p(full["peak_q"][held, point])
+    r2 = 1.0 - np.mean((pred[held, point] - truth) ** 2) / np.var(truth)
+    # one run after another, on a sample
+    sample = rng.choice(len(storms), size=args.plain_sample, replace=False)
+
+    def plain():
+        out = []
+        for i in sample:
+            m = Model(cat.tables, Numerics())
+            m.set_boundary(cat.boundary)
+            m.set_depth(np.zeros(cat.grid.shape))
+            tally = Tally(m, *cat.tally)
+            lines = Lines(m, [ln[:4] for ln in cat.lines])
+            rain = DeviceRain(m, storms[i], cat.rained)
+            run_windows(m, sim_h[i] * 3600.0, rain=rain, window=30.0, tally=tally)
+            out.append(float(lines.peaks()[0][point]))
+        return out
+
+    plain_q, plain_s = timed(plain)
+    same = all(plain_q[j] == full["peak_q"][i, point] for j, i in enumerate(sample))
+    plain_per_h = plain_s / sim_h[sample].sum()  # seconds of one-after-another solving per simulated hour
+    plain_sweep_s = plain_per_h * sim_h.sum()
+    line = {
+        "run": "configuration 5 critical-duration search", "cells": n * n, "dx_m": 10.0,
+        "candidates": len(storms), "design_points": len(cat.lines), "train_runs": int(args.train_runs),
+        "rerun_top": len(rerun), "setup_s": setup,
+        "exhaustive_batched": {"s": full_s, "runs_per_h": 3600.0 * len(storms) / full_s,
+                               "critical": crit, "peak_q": float(full["peak_q"][crit, point]),
+                               "duration_h": storms[crit].duration_h},
+        "screened": {"s": screen_s, "solver_s": tr_s + rr_s, "train_s": fit_s,
+                     "runs_per_h": 3600.0 * len(storms) / screen_s, "critical": found,
+                     "peak_q": solved[found], "same_critical": found == crit,
+                     "peak_q_error": solved[found] / float(full["peak_q"][crit, point]) - 1.0,
+                     "held_out_r2_log_peak": float(r2), "loss_first_last": [losses[0], losses[-1]]},
+        "naive_screen": {"critical": int(naive_found), "same_critical": int(naive_found) == crit,
+                         "peak_q_error": float(full["peak_q"][naive_found, point] / full["peak_q"][crit, point]) - 1.0},
+        "plain_one_after_another": {"sample": len(sample), "s_sample": plain_s, "s_per_simulated_h": plain_per_h,
+                                    "sweep_s_estimate": plain_sweep_s,
+                                    "runs_per_h": 3600.0 * len(storms) / plain_sweep_s, "same_peaks_as_batch": same},
+        "speedup_screened_vs_plain": plain_sweep_s / screen_s,
+        "speedup_batched_vs_plain": plain_sweep_s / full_s,
+    }  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     args = parse()
     if args.impl == "reference":
@@ -426,6 +532,9 @@ def main() -> None:
         return
     if args.ensemble:
         ensemble_run(args)
+        return
+    if args.critical:
+        critical_run(args)
         return
     import torch
     import torch.distributed as dist

@@ -261,8 +261,11 @@ def solve(cat: Catchment5, storms: list[MixedStorm], recession_h: float = 1.0, b
     q = np.zeros((len(storms), nl))
     tp = np.zeros((len(storms), nl))
     steps = np.zeros(len(storms), np.int64)
+    # batches of storms of like length: a batch steps until its longest run ends
+    by_length = np.argsort([s.duration_h for s in storms], kind="stable")
     for s0 in range(0, len(storms), batch):
-        part = storms[s0 : s0 + batch]
+        idx = by_length[s0 : s0 + batch]
+        part = [storms[i] for i in idx]
         n = len(part)
         B = Batch([cat.grid] * n, [cat.tables] * n, num)
         B.set_boundary([cat.boundary] * n)
@@ -274,8 +277,8 @@ def solve(cat: Catchment5, storms: list[MixedStorm], recession_h: float = 1.0, b
         B.run_windows(t_end, part, window=30.0, cells=cells)
         for r in range(n):
             pk, tt = B.line_peaks(r)
-            q[s0 + r], tp[s0 + r] = pk, tt / 3600.0
-        steps[s0 : s0 + n] = B.nsteps
+            q[idx[r]], tp[idx[r]] = pk, tt / 3600.0
+        steps[idx] = B.nsteps
         del B
     return {"peak_q": q, "t_peak_h": tp, "steps": steps}
 

@@ -22,6 +22,7 @@ cudaError_t update_setup();
 int update_occupancy();
 void launch_update(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s);
 __global__ void boundary_kernel(StepArgs A, int control);
+__global__ void clock_kernel(StepArgs A);
 __global__ void prestep_kernel(StepArgs A);
 __global__ void setstep_kernel(StepArgs A, float dtf, int want_wave, int want_wet, int nact);
 __global__ void endstep_kernel(StepArgs A);
@@ -236,6 +237,19 @@ static void drop_graphs(Handle& H) {
     H.loop.version = ~0u;
 }
 
+// CTAs of boundary_kernel: enough for its items (boundary cells; with control, tally faces and a warp a line), at
+// most four a SM.
+static int boundary_grid(const Handle& H, int control) {
+    int64_t items = H.nb;
+    if (control) {
+        items = items > H.ntally ? items : H.ntally;
+        items = items > (int64_t)H.nlines * 32 ? items : (int64_t)H.nlines * 32;
+    }
+    int64_t g = (items + 255) / 256;
+    const int64_t cap = 4 * (int64_t)(H.sms > 0 ? H.sms : 148);
+    return (int)(g < 1 ? 1 : (g > cap ? cap : g));
+}
+
 // One step of the device loop: every running run advances by one of its own steps.
 static int launch_loop_step(Handle& H, cudaStream_t s) {
     StepArgs A = make_args(H);
@@ -245,7 +259,8 @@ static int launch_loop_step(Handle& H, cudaStream_t s) {
     prestep_kernel<<<1, 1024, 0, s>>>(A);
     launch_faces(H.tmaps, A, faces_grid(H, H.g.ntiles - 1), s);
     launch_update(H.tmaps, A, grid, s);
-    boundary_kernel<<<1, 256, 0, s>>>(A, 1);
+    boundary_kernel<<<boundary_grid(H, 1), 256, 0, s>>>(A, 1);
+    clock_kernel<<<1, 256, 0, s>>>(A);
     activity_kernel<<<1, 1024, 0, s>>>(A, 0);
     plan_kernel<<<grid, blk, 0, s>>>(A, A.woken, -1);
     CKL("loop step");
@@ -447,7 +462,7 @@ int32_t w2b_step(void* handle, float dt, int32_t want_wave, int32_t want_wet, vo
     const int grid = blocks_for(*H, H->nact);
     launch_faces(H->tmaps, A, faces_grid(*H, H->nact), s);
     launch_update(H->tmaps, A, grid, s);
-    if (H->nb) boundary_kernel<<<1, 256, 0, s>>>(A, 0);
+    if (H->nb) boundary_kernel<<<boundary_grid(*H, 0), 256, 0, s>>>(A, 0);
     endstep_kernel<<<1, 1, 0, s>>>(A);
     CKL("w2b_step");
     H->cur ^= 1;
@@ -470,7 +485,7 @@ int32_t w2b_step_timed(void* handle, float dt, int32_t want_wave, int32_t want_w
     CK(cudaEventRecord(ev[1], s));
     launch_update(H->tmaps, A, grid, s);
     CK(cudaEventRecord(ev[2], s));
-    if (H->nb) boundary_kernel<<<1, 256, 0, s>>>(A, 0);
+    if (H->nb) boundary_kernel<<<boundary_grid(*H, 0), 256, 0, s>>>(A, 0);
     endstep_kernel<<<1, 1, 0, s>>>(A);
     CK(cudaEventRecord(ev[3], s));
     CKL("w2b_step_timed");

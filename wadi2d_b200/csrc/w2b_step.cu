@@ -648,19 +648,22 @@ void launch_update(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s) 
 
 // ------------------------------------------------------------------ boundary, tally, control (one CTA)
 
-// Boundary cells of every running run (wadi2d/solver/gpu/kernels/cells.cu:95-111), their envelope entries after the
-// overwrite, and, in the device loop (control = 1), the FP64 tally of every step and each run's clock after its step
-// (wadi2d/solver/stepper.py:113-124). One CTA.
+// Boundary cells of every running run (wadi2d/solver/gpu/kernels/cells.cu:95-111) and their envelope entries after
+// the overwrite; in the device loop (control = 1) also the FP64 tally of every step and the design lines. Every item
+// is independent of the others (a follow boundary reads an interior cell), so the kernel is a grid-stride loop over
+// them: boundary cells, then tally faces, then one warp a line.
 __global__ void boundary_kernel(StepArgs A, int control) {
     Ctl* ctl = A.ctl;
     if (!(ctl->any & ANY_RUN)) return;
     const RunTab& R = A.R;
-    const int tid = threadIdx.x;
-    for (int m = tid; m < A.nb; m += blockDim.x) {
+    const int gtid = blockIdx.x * blockDim.x + threadIdx.x, gstride = gridDim.x * blockDim.x;
+    for (int m = gtid; m < A.nb; m += gstride) {
         const int k = A.bcell[m];
         const int run = A.tile_run[tile_of_native(A, k)];
-        if (!(R.flags[run] & F_RUN)) continue;
-        float* h_next = A.hh[1 - R.parity[run]];
+        const int flags = R.flags[run];
+        if (!(flags & F_RUN)) continue;
+        const int n = 1 - R.parity[run];
+        float* h_next = A.hh[n];
         const int kind = A.bkind[m];
         if (kind == 0) {
             h_next[k] = A.bh0[m];
@@ -673,19 +676,12 @@ __global__ void boundary_kernel(StepArgs A, int control) {
             h_next[k] = h_next[r];
             A.d[k] = fmax32(A.d[r] + A.bd0[m], 0.0f);
         }
-    }
-    __syncthreads();
-    for (int m = tid; m < A.nb; m += blockDim.x) {
-        const int k = A.bcell[m];
-        const int run = A.tile_run[tile_of_native(A, k)];
-        const int n = 1 - R.parity[run];
-        if ((R.flags[run] & (F_RUN | F_MAX)) == (F_RUN | F_MAX))
-            envelope(A, fid_of_native(A, k), k, A.d[k], A.hh[n][k], R.max_time[run], ctl->arrive, ctl->deep,
+        if ((flags & F_MAX) == F_MAX)
+            envelope(A, fid_of_native(A, k), k, A.d[k], h_next[k], R.max_time[run], ctl->arrive, ctl->deep,
                      A.uu[0][n], A.uu[1][n]);
     }
     if (!control) return;
-    __syncthreads();
-    for (int m = tid; m < A.ntally; m += blockDim.x) {
+    for (int m = gtid; m < A.ntally; m += gstride) {
         const int face = A.tface[m];
         const int run = A.tile_run[tile_of_native(A, face)];
         if (!(R.flags[run] & F_RUN)) continue;
@@ -694,8 +690,9 @@ __global__ void boundary_kernel(StepArgs A, int control) {
     }
     // design lines (wadi2d/engine/monitor.py:229-232 at every step): Q = sum of sign q over the line's faces, FP64,
     // lane-strided then a fixed shuffle tree; the running peak of |Q| and the time at the end of the step
-    const int lane = tid & 31, nwarps = blockDim.x >> 5;
-    for (int l = tid >> 5; l < A.nlines; l += nwarps) {
+    const int lane = threadIdx.x & 31;
+    const int gwarp = gtid >> 5, nwarps = gstride >> 5;
+    for (int l = gwarp; l < A.nlines; l += nwarps) {
         const int s = A.lstart[l], e = A.lstart[l + 1];
         if (s >= e) continue;
         const int run = A.tile_run[tile_of_native(A, A.lface[s])];
@@ -715,8 +712,16 @@ __global__ void boundary_kernel(StepArgs A, int control) {
             }
         }
     }
-    __syncthreads();
-    for (int r = tid; r < A.nruns; r += blockDim.x) {
+}
+
+// Each running run's clock after its step (wadi2d/solver/stepper.py:113-124): the swap of its halves, t, the step
+// counts, the step rule on refresh steps (dt_min and non-finite checks); a run that stops marks the work list for
+// rebuilding. One CTA, after boundary_kernel.
+__global__ void clock_kernel(StepArgs A) {
+    Ctl* ctl = A.ctl;
+    if (!(ctl->any & ANY_RUN)) return;
+    const RunTab& R = A.R;
+    for (int r = threadIdx.x; r < A.nruns; r += blockDim.x) {
         if (!(R.flags[r] & F_RUN)) continue;
         R.parity[r] ^= 1;
         R.t[r] = R.t[r] + R.dt_step[r];

@@ -65,6 +65,10 @@ def parse():
     p.add_argument("--recession-min", type=float, default=30.0, help="simulated time after each storm, minutes")
     p.add_argument("--time-scale", type=float, default=1.0, help="share of each run's simulated time to step")
     p.add_argument("--skip-plain", action="store_true", help="the batch only (no one-after-another sweep)")
+    p.add_argument("--config2-run", action="store_true",
+                   help="configuration 2 end to end: 1024 x 1024, crests, lumped inflows, a reservoir, 6 h")
+    p.add_argument("--table-build", action="store_true",
+                   help="the GPU table build of configuration 2 (1024 x 1024, 1 m pixels) and 3 (4096 x 4096, 7.5 m)")
     p.add_argument("--critical", action="store_true",
                    help="configuration 5: the critical-duration search, screened by the network, against the sweep")
     p.add_argument("--candidates", type=int, default=400, help="--critical: candidate storms")
@@ -522,6 +526,123 @@ def critical_run(args) -> None:
     print(json.dumps(line), flush=True)
 
 
+def config2_run(args) -> None:
+    """Configuration 2 end to end: 1024 x 1024 cells at 10 m, 10 x 10 pixels a cell (tables on the GPU), 40 breakline
+    crests, Manning patches, the 200 x 50 m reservoir started 4 m above its downstream bed (its depths through
+    hbar_at_level), three lumped inflows at the channel heads shared over their cells by depth each 30 s window
+    (wadi2d/forcing.py:667-695, depths read from the device), a free outfall on the south edge; 6 h on the device loop
+    with sleeping tiles, the envelope every 4 steps and the FP64 outfall tally every step; the books."""
+    import torch
+
+    from wadi2d_b200 import forcing as F
+    from wadi2d_b200 import workloads
+    from wadi2d_b200.backend import BoundaryCells
+    from wadi2d_b200.config import Numerics, Tables
+    from wadi2d_b200.grid import TileGrid
+    from wadi2d_b200.maxima import Maxima, Tally
+    from wadi2d_b200.model import Model
+    from wadi2d_b200.run import DeviceStorage, run_windows
+    from wadi2d_b200.state import state_index
+    from wadi2d_b200.tables import ArrayBed, build_tables, hbar_at_level
+
+    dev = torch.device("cuda", 0)
+    t0 = time.perf_counter()
+    n = 1024
+    c = workloads.crest_valley(n=n)
+    grid = TileGrid.from_mask(np.ones((n, n), bool), 0.0, 0.0, c.dx)
+    tables = build_tables(grid, ArrayBed(torch.as_tensor(c.z, device=dev), c.dx / c.k), Tables(), c.manning,
+                          crest=c.crest, device=dev)  # fmt: skip
+    del c.z
+    m = Model(tables, Numerics())
+    rows, cols = c.outfall
+    cells = state_index(grid, rows, cols).astype(np.int32)
+    nb = cells.size
+    m.set_boundary(BoundaryCells(cells, cells.copy(), np.ones(nb, np.int32), np.zeros(nb, np.float32),
+                                 np.zeros(nb, np.float32)))  # fmt: skip
+    rr, rc, level = c.reservoir
+    hc, dtab = grid.from_tiles(tables.hc), grid.from_tiles(tables.dtab)
+    zmin = np.asarray(tables.zmin)
+    h0 = np.zeros(grid.shape)
+    h0[rr, rc] = hbar_at_level(np.full(rr.size, level), zmin[rr, rc], hc[rr, rc], dtab[rr, rc])
+    m.set_depth(h0)
+    taken = np.zeros(grid.shape, bool)
+    taken[rows, cols] = True
+    inner = grid.mask & ~taken
+    jj, ii = np.nonzero(inner)
+    interior = state_index(grid, jj, ii).astype(np.int64)
+    (xf, xs), (yf, ys) = F.open_faces(grid, inner, taken)
+    tally = Tally(m, xf, xs, yf, ys)
+    maxima = Maxima(m, 0.1, 0.05, every=4)
+    pos = {int(k): p for p, k in enumerate(interior)}
+    injections = []
+    for q, (ir, icol, low, times, flows) in enumerate(c.inflows):
+        idx = state_index(grid, ir, icol).astype(np.int64)
+        injections.append(F.Injection(f"inflow {q}", np.array([pos[int(k)] for k in idx]), idx, low, times, flows,
+                                      0.1))  # fmt: skip
+    forcing = F.Forcing(interior, c.dx**2, injections=injections,
+                        depth_reader=lambda inj: m.read_cells("d", inj.index))  # fmt: skip
+    storage = DeviceStorage(m, interior)
+    setup = time.perf_counter() - t0
+    torch.cuda.synchronize(dev)
+    w0 = time.perf_counter()
+    out = run_windows(m, c.t_end, host_forcing=forcing, window=30.0, maxima=maxima, tally=tally, storage=storage)
+    torch.cuda.synchronize(dev)
+    wall = time.perf_counter() - w0
+    b = out.balance
+    env = maxima.fields()
+    qx, qy = m.field("qx"), m.field("qy")
+    crest_x = np.isfinite(c.crest.xz) & grid.mask
+    line = {
+        "run": "configuration 2, 6 h", "cells": n * n, "steps": out.steps, "windows": out.windows, "wall_s": wall,
+        "setup_s": setup, "cell_steps_per_s": n * n * out.steps / wall, "inflow_m3": b.inflow,
+        "reservoir_m3": b.storage0, "outflow_m3": b.outflow, "storage_m3": b.storage, "mass_error": b.relative,
+        "peak_depth_m": float(env["depth"].max()), "peak_speed_m_s": float(env["speed"].max()),
+        "wet_cells_end": int((m.field("h") > 0).sum()), "crest_x_faces": int(crest_x.sum()),
+        "crest_x_faces_flowing_end": int((crest_x & (qx != 0.0)).sum()),
+    }  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
+def table_build(args) -> None:
+    """The sub-grid tables built on the GPU (w2b_build_tables), timed with CUDA events: configuration 2 (1024 x 1024
+    cells at 10 m, 10 x 10 pixels a cell, 40 breakline crests, Manning patches; face lines of 298 pixels for the
+    local radius) and configuration 3 (4096 x 4096 at 30 m, 4 x 4 pixels; lines of 44 pixels)."""
+    import torch
+
+    from wadi2d_b200 import workloads
+    from wadi2d_b200.config import Tables
+    from wadi2d_b200.grid import TileGrid
+    from wadi2d_b200.tables import ArrayBed, build_tables
+
+    dev = torch.device("cuda", 0)
+    stream = torch.cuda.current_stream(dev)
+    out = {}
+    for name, make in (("configuration 2", lambda: workloads.crest_valley(n=1024)),
+                       ("configuration 3", lambda: workloads.catchment(n=4096, device=dev))):  # fmt: skip
+        g0 = time.perf_counter()
+        c = make()
+        gen = time.perf_counter() - g0
+        n = c.n
+        grid = TileGrid.from_mask(np.ones((n, n), bool), 0.0, 0.0, c.dx)
+        crest = getattr(c, "crest", None)
+        z = c.z if isinstance(c.z, torch.Tensor) else torch.as_tensor(c.z, device=dev)
+        small = TileGrid.from_mask(np.ones((62, 62), bool), 0.0, 0.0, c.dx)  # a first build, for the kernels' set-up
+        build_tables(small, ArrayBed(z[: 64 * c.k, : 64 * c.k], c.dx / c.k), Tables(), 0.035, device=dev)
+        torch.cuda.synchronize(dev)
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        tables = build_tables(grid, ArrayBed(z, c.dx / c.k), Tables(), c.manning, crest=crest, device=dev)
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        ms = e0.elapsed_time(e1)
+        out[name] = {"cells": n * n, "pixels_per_cell": c.k * c.k, "pixel_m": c.dx / c.k, "build_s": ms / 1e3,
+                     "cells_per_s": n * n / (ms / 1e3), "generate_s": gen,
+                     "rows": tables.rows}  # fmt: skip
+        del tables, z, c
+        torch.cuda.empty_cache()
+    print(json.dumps({"run": "GPU table build", **out}), flush=True)
+
+
 def main() -> None:
     args = parse()
     if args.impl == "reference":
@@ -535,6 +656,12 @@ def main() -> None:
         return
     if args.critical:
         critical_run(args)
+        return
+    if args.table_build:
+        table_build(args)
+        return
+    if args.config2_run:
+        config2_run(args)
         return
     import torch
     import torch.distributed as dist

@@ -279,7 +279,9 @@ typedef struct {
 int64_t w2b_table_workspace_doubles(int32_t nmax, int64_t threads);
 
 /* Replaces build_tables (wadi2d/tables/builder.py:131-258): cell tables, face tables (strips, or the local
- * hydraulic radius when local != 0), centre beds, inverts, closed faces and natural crests, on the GPU. */
+ * hydraulic radius when local != 0), centre beds, inverts, closed faces and natural crests, on the GPU. The local
+ * radius works in shared memory when a face's line (k + 2 margin pixels) is at most about 2,800 pixels, and in
+ * out->ws beyond that; out->ws is required with local != 0 either way. */
 int32_t w2b_build_tables(const W2BTableIn* in, const W2BTableOut* out, void* stream);
 
 /* w2b_build_tables for callers that cannot allocate device memory. It has no counterpart in the reference. A
@@ -289,7 +291,7 @@ int32_t w2b_build_tables(const W2BTableIn* in, const W2BTableOut* out, void* str
  * allocating library call) and uses instead a 32 MiB array of file-scope device memory, which every GPU that loads
  * the library holds until the process exits. out->ws and out->ws_threads are ignored.
  *  - Limit: a face's line (k + 2 margin pixels) of at most 3,639 pixels; longer lines are refused with W2B_EINVAL
- *    and a message. Fewer threads fit the fixed scratch than the caller-scratch entry point uses, so it is slower.
+ *    and a message. Lines that fit the builder's shared-memory workspace (about 2,800 pixels) do not touch the array.
  *  - The first call on a device looks the array's address up (cudaGetSymbolAddress) with that device current;
  *    make that first call before any stream capture.
  *  - Every call shares the one array and it keeps the last call's contents; the kernels write every scratch slot

@@ -318,14 +318,19 @@ __device__ void local_radius(const Work& W, int n, int i0, int i1, double zf, do
 }
 
 constexpr int KMAX = 32;
+constexpr int64_t FACE_SMEM_BYTES = 200 * 1024;  // the shared workspace a CTA of the face-table kernel may take
 constexpr int ROWS_MAX = 64;
 
+// SMEM: the local radius's workspace in this CTA's shared memory (interleaved across its threads as the global one is
+// across the grid's), else in the caller's device workspace. The arithmetic is the same either way.
+template <bool SMEM>
 __global__ void __launch_bounds__(128) face_tables_kernel(TableArgs A) {
+    extern __shared__ double sws[];
     const int64_t nface = (int64_t)(A.ntiles - 1) * TILE2 * 2;
     const int k = A.k, rows = A.rows;
     double prof[KMAX], weight[KMAX], tab[2 * ROWS_MAX];
     const int64_t tid = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const Work W{A.ws, A.ws_threads, tid, A.nmax};
+    const Work W = SMEM ? Work{sws, (int64_t)blockDim.x, (int64_t)threadIdx.x, A.nmax} : Work{A.ws, A.ws_threads, tid, A.nmax};
     for (int64_t f = tid; f < nface; f += (int64_t)gridDim.x * blockDim.x) {
         const int axis = (int)(f & 1);
         const int64_t c = f >> 1;
@@ -508,8 +513,27 @@ int32_t w2b_build_tables(const W2BTableIn* in, const W2BTableOut* out, void* str
         cell_tables_kernel<256><<<cblocks, 128, 0, s>>>(A);
     else
         cell_tables_kernel<1024><<<cblocks, 128, 0, s>>>(A);
-    const int64_t fthreads = in->local ? out->ws_threads : (int64_t)148 * 8 * 128;
-    face_tables_kernel<<<(unsigned)(fthreads / 128), 128, 0, s>>>(A);
+    // the local radius's workspace: in shared memory when a CTA of at least one thread fits it (a face line of up to
+    // about 2,800 pixels), else in the caller's workspace
+    const int64_t per_thread = 9 * (int64_t)(A.nmax + 1) * (int64_t)sizeof(double);
+    const int64_t smem_threads = in->local ? FACE_SMEM_BYTES / per_thread : 0;
+    if (in->local && smem_threads >= 1) {
+        const int threads = smem_threads > 128 ? 128 : (int)smem_threads;
+        const size_t bytes = (size_t)threads * (size_t)per_thread;
+        int dev = 0, sms = 148;
+        cudaGetDevice(&dev);
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        if (cudaFuncSetAttribute(face_tables_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) !=
+            cudaSuccess) {
+            fprintf(stderr, "libwadi_b200: w2b_build_tables: shared workspace: %s\n",
+                    cudaGetErrorString(cudaGetLastError()));
+            return W2B_ECUDA;
+        }
+        face_tables_kernel<true><<<sms, threads, bytes, s>>>(A);
+    } else {
+        const int64_t fthreads = in->local ? out->ws_threads : (int64_t)148 * 8 * 128;
+        face_tables_kernel<false><<<(unsigned)(fthreads / 128), 128, 0, s>>>(A);
+    }
     close_faces_kernel<<<148 * 8, 256, 0, s>>>(A);
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {

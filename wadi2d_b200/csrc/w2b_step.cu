@@ -1,10 +1,11 @@
 // The uniform-grid step on sm_100a: face pass, update pass (positivity ratio, continuity, level lookup, envelope),
 // boundary/tally/control pass, active-list rebuild, and the layout converters.
 //
-// One CTA of 256 threads (32 x 8) takes one 32 x 32 tile at a time, looping over the active list (grid-stride, so a
-// graph-captured launch serves any list length). Each thread owns one column and four rows of the tile. State sits
-// in the dense NATIVE layout, so a neighbour is an address offset and the reference's halo exchanges
-// (wadi2d/solver/gpu/kernels/cells.cu:80-93) disappear; the guard ring is zero like the reference's void tile.
+// A CTA takes one 32 x 32 tile at a time, looping over its share of the work list (grid-stride, so a graph-captured
+// launch serves any list length): the face pass with 512 threads (a thread a column, two rows), the update pass with
+// 256 (a thread a column, four rows). State sits in the dense NATIVE layout, so a neighbour is an address offset and
+// the reference's halo exchanges (wadi2d/solver/gpu/kernels/cells.cu:80-93) disappear; the guard ring is zero like
+// the reference's void tile. In a batch every tile reads its run's clock, cell size, flags and current half.
 //
 // The face pass restates wadi2d/solver/gpu/kernels/faces.cu:10-175 (= wadi2d/solver/cpu/kernels.py:86-244); the
 // update pass fuses limit and update (cells.cu:4-63, kernels.py:247-299) by computing the positivity ratio r of the
@@ -255,10 +256,11 @@ __device__ __forceinline__ float block_max(float v, float* red) {
     return r;
 }
 
-// The face pass: both own faces of every cell of the active tiles (wadi2d/solver/gpu/kernels/faces.cu:148-175).
-// Each CTA (16 warps, a warp a tile row, two rows a warp) stages a tile with TMA: nine 40 x 36 state boxes, the two
-// momenta, and the tile's twelve static face scalars as bulk copies; the per-tile wave maxima are reduced at the end
-// by the last CTA to finish. p is the parity of the ping-pong halves.
+// The face pass: both own faces of every cell of the tiles of the work list (wadi2d/solver/gpu/kernels/faces.cu:
+// 148-175). Each CTA (16 warps, a warp a tile row, two rows a warp; two CTAs a SM) stages a tile with TMA: nine
+// 40 x 36 state boxes, the two momenta, and the tile's twelve static face scalars as bulk copies; on refresh steps
+// the tile's wave maximum goes to its run's maximum (an integer atomic max on the float bits). p is the parity of
+// the run's ping-pong halves.
 __global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_constant__ TMaps M, StepArgs A) {
     extern __shared__ __align__(128) float sm[];
     __shared__ __align__(8) uint64_t bar;

@@ -29,51 +29,67 @@ constexpr int SM_FLOATS = SM_ST + 12 * TILE2;
 constexpr int FACES_SMEM = SM_FLOATS * 4;  // 109,184 bytes: two CTAs a SM
 constexpr int FACES_THREADS = 512;
 
-// What the first part of a face computes: the upwind choice, the face depth, the table row, and the row's quad,
-// whose load is issued there and consumed after the table-free momentum terms.
+// What the first part of a face hands to the rest: the row's quad (its load is issued in part A and consumed after
+// the table-free momentum terms), the face depth, and the table row with the upwind choice, the live flag and the
+// above-the-table flag packed in one word. Parts B and C re-read the other inputs from the tile's image, so few
+// registers stay live across the momentum terms.
 struct FaceA {
-    float e_l, e_r, e_lp, e_rp, uf, eup, eface, top, cwf, fl, fr;
-    int r;
-    bool from_left, live, above;
     float4 q;
+    float eface;
+    int bits;
 };
+constexpr int FA_ROW = 0xff, FA_LEFT = 0x100, FA_LIVE = 0x200, FA_ABOVE = 0x400;
+
+// The face's upwind inputs from the tile's image (wadi2d/solver/gpu/kernels/faces.cu:19-31): the levels over each
+// side's invert, their positive parts, and the velocity on the face.
+struct FaceIn {
+    float e_l, e_r, e_lp, e_rp, uf;
+};
+template <int AX>
+__device__ __forceinline__ FaceIn face_in(const float* sm, int b, int local) {
+    constexpr int S = AX == 0 ? 1 : BOXW;
+    const float* D = sm + F_D * BOX;
+    const float* U = sm + (AX == 0 ? F_U : F_V) * BOX;
+    const float* st = sm + SM_ST + AX * 6 * TILE2;
+    FaceIn I;
+    I.e_l = D[b - S] - st[0 * TILE2 + local];
+    I.e_r = D[b] - st[1 * TILE2 + local];
+    I.uf = U[b];
+    I.e_lp = fmax32(I.e_l, 0.0f);
+    I.e_rp = fmax32(I.e_r, 0.0f);
+    return I;
+}
 
 // Part A of the face of axis AX at box index b (wadi2d/solver/gpu/kernels/faces.cu:19-44).
 template <int AX>
 __device__ __forceinline__ void face_a(const float* sm, int b, int local, const StepArgs& A, int t, FaceA& F) {
     constexpr int S = AX == 0 ? 1 : BOXW;
     const W2BParams& P = A.P;
-    const float* D = sm + F_D * BOX;
-    const float* U = sm + (AX == 0 ? F_U : F_V) * BOX;
     const float* st = sm + SM_ST + AX * 6 * TILE2;
-    F.fl = st[0 * TILE2 + local];
-    F.fr = st[1 * TILE2 + local];
-    F.e_l = D[b - S] - F.fl;
-    F.e_r = D[b] - F.fr;
-    F.uf = U[b];
-    F.e_lp = fmax32(F.e_l, 0.0f);
-    F.e_rp = fmax32(F.e_r, 0.0f);
-    F.from_left = F.uf > 0.0f || (F.uf == 0.0f && F.e_l >= F.e_r);
-    F.eup = F.from_left ? F.e_lp : F.e_rp;
-    F.live = !(F.eup <= P.e_wet);
-    if (!F.live) return;
-    F.cwf = st[5 * TILE2 + local];
-    F.top = st[4 * TILE2 + local];
-    F.eface = F.eup;
-    if (P.carry && F.cwf == 0.0f) {
+    const FaceIn I = face_in<AX>(sm, b, local);
+    const bool from_left = I.uf > 0.0f || (I.uf == 0.0f && I.e_l >= I.e_r);
+    const float eup = from_left ? I.e_lp : I.e_rp;
+    F.bits = from_left ? FA_LEFT : 0;
+    if (eup <= P.e_wet) return;
+    const float cwf = st[5 * TILE2 + local];
+    const float top = st[4 * TILE2 + local];
+    float eface = eup;
+    if (P.carry && cwf == 0.0f) {
         const float* ZC = sm + (AX == 0 ? F_ZCX : F_ZCY) * BOX;
-        const float dz = F.from_left ? ZC[b - S] - F.fl : ZC[b] - F.fr;
+        const float dz = from_left ? ZC[b - S] - st[0 * TILE2 + local] : ZC[b] - st[1 * TILE2 + local];
         if (dz > 1e-6f) {
-            float phi = (F.eup - 2.0f * dz) / (2.0f * dz);
+            float phi = (eup - 2.0f * dz) / (2.0f * dz);
             phi = phi < 0.0f ? 0.0f : (phi > 1.0f ? 1.0f : phi);
-            F.eface = F.eup - phi * dz;
+            eface = eup - phi * dz;
         }
     }
     const int last = A.rows - 1;
-    F.above = F.eface >= F.top;
-    F.r = F.above ? last - 1 : row_of(sqrtf(F.eface / F.top) * (float)last, last);
+    const bool above = eface >= top;
+    const int r = above ? last - 1 : row_of(sqrtf(eface / top) * (float)last, last);
+    F.eface = eface;
+    F.bits |= FA_LIVE | (above ? FA_ABOVE : 0) | r;
     const float4* quads = A.ftab4[AX] + (size_t)t * (A.rows - 1) * TILE2 + local;
-    F.q = __ldg(quads + (size_t)F.r * TILE2);
+    F.q = __ldg(quads + (size_t)r * TILE2);
 }
 
 // Parts B and C: the momentum terms (faces.cu:50-100, table-free), then the lookup, section, friction, crest cap,
@@ -86,7 +102,7 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
     constexpr int S = AX == 0 ? 1 : BOXW;
     constexpr int PP = AX == 0 ? BOXW : 1;
     const W2BParams& P = A.P;
-    if (!F.live) {
+    if (!(F.bits & FA_LIVE)) {
         if constexpr (PROBE) {
             probe_un[local] = 0.0f;
         } else {
@@ -104,22 +120,24 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
     const float* Q = sm + (AX == 0 ? F_QX : F_QY) * BOX;
     const float* QP = sm + (AX == 0 ? F_QY : F_QX) * BOX;
     const float* st = sm + SM_ST + AX * 6 * TILE2;
-    const bool from_left = F.from_left;
-    const float uf = F.uf;
+    const FaceIn I = face_in<AX>(sm, b, local);
+    const bool from_left = (F.bits & FA_LEFT) != 0;
+    const float uf = I.uf;
+    const float eup = from_left ? I.e_lp : I.e_rp;
     const float h_l = H[b - S], h_r = H[b];
     const float hup = from_left ? h_l : h_r;
 
     // [1] section: the disconnected drive (the volume-limited section needs the table, below)
-    float d_eta = F.e_rp - F.e_lp;
+    float d_eta = I.e_rp - I.e_lp;
     if (P.sheet) {
-        const float edown = from_left ? F.e_rp : F.e_lp;
+        const float edown = from_left ? I.e_rp : I.e_lp;
         if (edown <= ZERO) {
             const float g_u = from_left ? st[2 * TILE2 + local] : st[3 * TILE2 + local];
             const float g_d = from_left ? st[3 * TILE2 + local] : st[2 * TILE2 + local];
             const float h_d = from_left ? h_r : h_l;
             const float drop = (hup - g_u) - fmax32(h_d - g_d, HALF * (g_u - g_d));
-            const float level_drop = fabsf(F.e_l - F.e_r);
-            const float drive = fmax32(F.eup, fmin32(drop, level_drop));
+            const float level_drop = fabsf(I.e_l - I.e_r);
+            const float drive = fmax32(eup, fmin32(drop, level_drop));
             d_eta = from_left ? -drive : drive;
         }
     }
@@ -160,16 +178,16 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
     // the table lookup from the quad loaded in part A (common.cuh face_lookup); rowc holds, per row r, c0^2 and
     // c1^2 - c0^2 with c0 = r / m, c1 = (r + 1) / m, and in its last slot 1 - c^2 with c = (m - 1) / m: the very
     // float32 values the lookup forms, computed once a CTA
-    const float top = F.top, e = F.eface;
+    const float top = st[4 * TILE2 + local], e = F.eface;
     const float4 q = F.q;
     float area, tt, w;
-    if (F.above) {
+    if (F.bits & FA_ABOVE) {
         const float a1 = q.z, a0 = q.x;
         w = (a1 - a0) / (top * rowc[2 * (A.rows - 1)]);
         area = a1 + w * (e - top);
         tt = q.w * (area / fmax32(a1, 1e-12f));
     } else {
-        const int r = F.r;
+        const int r = F.bits & FA_ROW;
         const float e0 = rowc[2 * r] * top;
         const float de = rowc[2 * r + 1] * top;
         const float f = (e - e0) / de;
@@ -182,7 +200,7 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
     if (P.sheet) {
         const float avol = hup * dx;
         if (avol < area) {
-            const float sub = fmin32(F.e_lp, F.e_rp) / fmax32(F.e_lp, F.e_rp);
+            const float sub = fmin32(I.e_lp, I.e_rp) / fmax32(I.e_lp, I.e_rp);
             const float sub2 = sub * sub;
             const float alpha = sub2 * sub2;
             rho = alpha + (ONE - alpha) * avol / area;
@@ -198,7 +216,7 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
     if (fabsf(un) > P.u_max) un = un > ZERO ? P.u_max : -P.u_max;
     // [6] crest face
     float qn = area * rho * un;
-    float c = F.cwf;
+    float c = st[5 * TILE2 + local];
     if (c != ZERO) {
         float area_c = area, w_c = w;
         if (c < ZERO) {
@@ -206,7 +224,7 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
             const float ua = from_left ? um : up;
             float tc;
             const float4* quads = A.ftab4[AX] + (size_t)t * (A.rows - 1) * TILE2 + local;
-            face_lookup(F.eup + HALF * ua * ua / P.g, top, quads, A.rows, area_c, tc, w_c);
+            face_lookup(eup + HALF * ua * ua / P.g, top, quads, A.rows, area_c, tc, w_c);
         }
         const float qc = c * area_c * sqrtf(area_c / fmax32(w_c, 1e-9f));
         if (fabsf(qn) > qc) {

@@ -776,7 +776,7 @@ def main() -> None:
                        "l2": "inputs larger than L2 (about 15 GB resident)", "parallelism": f"replicas x{world}",
                        "loop": "device-resident, CUDA graphs of 16 steps"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-            "gpu_launches": 7 * ran,
+            "gpu_launches": 8 * ran,
         }  # fmt: skip
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -22,6 +22,7 @@ cudaError_t update_setup();
 int update_occupancy();
 void launch_update(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s);
 __global__ void boundary_kernel(StepArgs A, int control);
+__global__ void envelope_kernel(StepArgs A);
 __global__ void clock_kernel(StepArgs A);
 __global__ void prestep_kernel(StepArgs A);
 __global__ void setstep_kernel(StepArgs A, float dtf, int want_wave, int want_wet, int nact);
@@ -259,6 +260,7 @@ static int launch_loop_step(Handle& H, cudaStream_t s) {
     prestep_kernel<<<1, 1024, 0, s>>>(A);
     launch_faces(H.tmaps, A, faces_grid(H, H.g.ntiles - 1), s);
     launch_update(H.tmaps, A, grid, s);
+    envelope_kernel<<<H.sms * 2, TILE2, 0, s>>>(A);
     boundary_kernel<<<boundary_grid(H, 1), 256, 0, s>>>(A, 1);
     clock_kernel<<<1, 256, 0, s>>>(A);
     activity_kernel<<<1, 1024, 0, s>>>(A, 0);
@@ -315,6 +317,16 @@ int32_t w2b_create(const W2BGridDesc* grid, const W2BParams* params, const W2BBu
     if (!grid || !params || !buffers || !handle) return W2B_EINVAL;
     if (grid->rows < 4 || grid->rows > 64 || grid->nruns < 1) return W2B_EINVAL;
     if (!buffers->runs || ((uintptr_t)buffers->runs & 255) || !buffers->tile_run || !buffers->work) return W2B_EINVAL;
+    {
+        // arrays the passes stage with bulk copies: 16-byte aligned
+        auto a16 = [](const void* q) { return q && !((uintptr_t)q & 15); };
+        bool ok = a16(buffers->hc);
+        for (int x = 0; x < 2; ++x)
+            ok = ok && a16(buffers->fl[x]) && a16(buffers->fr[x]) && a16(buffers->gl[x]) && a16(buffers->gr[x]) &&
+                 a16(buffers->ef[x]) && a16(buffers->cw[x]);
+        for (int e = 0; e < 5; ++e) ok = ok && a16(buffers->env[e]);
+        if (!ok) return W2B_EINVAL;
+    }
     Handle* H = new (std::nothrow) Handle();
     if (!H) return W2B_EINVAL;
     H->g = *grid;

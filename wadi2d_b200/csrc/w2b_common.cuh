@@ -34,7 +34,7 @@ struct Ctl {
 };
 static_assert(sizeof(Ctl) <= W2B_CTL_BYTES, "control block too large");
 
-constexpr uint32_t ANY_RUN = 1u, ANY_WAVE = 2u, ANY_ACT = 4u;
+constexpr uint32_t ANY_RUN = 1u, ANY_WAVE = 2u, ANY_ACT = 4u, ANY_MAX = 8u;
 // per-run flags of this step
 constexpr int32_t F_RUN = 1, F_WAVE = 2, F_WET = 4, F_MAX = 8, F_ACT = 16;
 

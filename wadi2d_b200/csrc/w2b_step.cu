@@ -1,4 +1,4 @@
-// The uniform-grid step on sm_100a: face pass, update pass (positivity ratio, continuity, level lookup, envelope),
+// The uniform-grid step on sm_100a: face pass, update pass (positivity ratio, continuity, level lookup), envelope pass,
 // boundary/tally/control pass, active-list rebuild, and the layout converters.
 //
 // A CTA takes one 32 x 32 tile at a time, looping over its share of the work list (grid-stride, so a graph-captured
@@ -464,30 +464,6 @@ void launch_faces(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s) {
 
 __device__ __forceinline__ float scaled(float q, float rl, float rr) { return q * (q > 0.0f ? rl : rr); }
 
-// Envelope of one own cell, wadi2d/engine/maxima.py:75-92 (the CPU twin forms the centre speed in float64).
-// un, vn: the face velocities after the step.
-__device__ __forceinline__ void envelope(const StepArgs& A, int fid, int k, float dk, float hk, float time,
-                                         float arrive, float deep, const float* un, const float* vn) {
-    float* __restrict__ dmax = A.env[0];
-    float* __restrict__ hmax = A.env[1];
-    float* __restrict__ smax = A.env[2];
-    float* __restrict__ zmax = A.env[3];
-    float* __restrict__ tarr = A.env[4];
-    dmax[fid] = fmax32(dmax[fid], dk);
-    hmax[fid] = fmax32(hmax[fid], hk);
-    if (dk > deep) {
-        const double uc = 0.5 * (double)(un[k] + un[k + 1]);
-        const double vc = 0.5 * (double)(vn[k] + vn[k + A.px]);
-        const double s = sqrt(uc * uc + vc * vc);
-        const double sm = (double)smax[fid];
-        smax[fid] = (float)(sm >= s ? sm : s);
-        const double hz = s * (double)dk;
-        const double zm = (double)zmax[fid];
-        zmax[fid] = (float)(zm >= hz ? zm : hz);
-    }
-    if (tarr[fid] < 0.0f && dk >= arrive) tarr[fid] = time;
-}
-
 constexpr int RING = TILE + 2;  // the tile and its one-cell ring
 constexpr int RPAD = RING + 1;
 constexpr int U_QX1 = 0, U_QY1 = 1, U_H = 2;       // 40 x 36 boxes
@@ -500,14 +476,13 @@ constexpr int UPDATE_THREADS = 256;
 // The update pass (wadi2d/solver/gpu/kernels/cells.cu:4-63 with limit fused in): TMA stages the tile's unscaled
 // discharges and old depth with their ring, its residual, source and Hc; r of the tile and its one-cell ring is
 // formed in shared memory; then each thread takes its four cells through continuity, issues their four level-table
-// loads together, and finishes the level, the wet share, the wet flag and, on envelope steps, the envelope.
+// loads together, and finishes the level, the wet share and the wet flag.
 __global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_constant__ TMaps M, StepArgs A) {
     extern __shared__ __align__(128) float sm[];
     __shared__ __align__(8) uint64_t bar;
     Ctl* ctl = A.ctl;
     if (!(ctl->any & ANY_RUN)) return;
     const int nwork = ctl->nwork;
-    const float arrive = ctl->arrive, deep = ctl->deep;
     const int px = A.px;
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
     const int rows = A.rows, last = rows - 1;
@@ -535,8 +510,6 @@ __global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_con
         const float area = dxr * dxr;
         const int want_plan = (flags & F_WAVE) != 0;
         const int want_wet = (flags & F_WET) != 0;
-        const int want_max = (flags & F_MAX) != 0;
-        const float time = A.R.max_time[run];
         const int p = A.R.parity[run];
         float* __restrict__ h_next = A.hh[1 - p];
         const int tj = A.tiles[2 * t], ti = A.tiles[2 * t + 1];
@@ -640,8 +613,6 @@ __global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_con
             A.d[k] = dk;
             if (want_plan) A.om[k] = om;
             any |= h > 0.0f;
-            if (want_max && !((A.bmark[t * TILE + jj] >> ii) & 1u))
-                envelope(A, t * TILE2 + local, k, dk, h, time, arrive, deep, A.uu[0][1 - p], A.uu[1][1 - p]);
         }
         if (want_wet) {
             const int w = __syncthreads_or(any);
@@ -664,6 +635,51 @@ int update_occupancy() {
 
 void launch_update(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s) {
     update_kernel<<<grid, dim3(32, 8), UPDATE_SMEM, s>>>(M, A);
+}
+
+// ------------------------------------------------------------------ envelope pass
+
+// The envelope of one own cell (wadi2d/engine/maxima.py:75-92; the CPU twin forms the centre speed in float64) with
+// every load issued before any store, so that a thread's loads make one round trip; only the entries that change are
+// written. un, vn: the face velocities after the step.
+__device__ __forceinline__ void envelope_cell(const StepArgs& A, int fid, int k, float dk, float hk, float time,
+                                              float arrive, float deep, const float* un, const float* vn) {
+    const float d0 = A.env[0][fid], h0 = A.env[1][fid], s0 = A.env[2][fid], z0 = A.env[3][fid];
+    const float a0 = A.env[4][fid];
+    const float ue = un[k + 1], uw = un[k], vs = vn[k + A.px], vn0 = vn[k];
+    // max(old, new) as fmax32 forms it keeps old exactly when old >= new
+    if (!(d0 >= dk)) A.env[0][fid] = dk;
+    if (!(h0 >= hk)) A.env[1][fid] = hk;
+    if (dk > deep) {
+        const double uc = 0.5 * (double)(uw + ue);
+        const double vc = 0.5 * (double)(vn0 + vs);
+        const double sp = sqrt(uc * uc + vc * vc);
+        if (!((double)s0 >= sp)) A.env[2][fid] = (float)sp;
+        const double hz = sp * (double)dk;
+        if (!((double)z0 >= hz)) A.env[3][fid] = (float)hz;
+    }
+    if (a0 < 0.0f && dk >= arrive) A.env[4][fid] = time;
+}
+
+// The envelope after a step of the device loop, for the own cells of the work list's tiles whose runs record it at
+// this step (F_MAX); boundary cells are recorded by the boundary pass after its overwrite. A CTA a tile at a time, a
+// thread a cell; on steps that record no envelope every CTA returns at once.
+__global__ void __launch_bounds__(TILE2, 2) envelope_kernel(StepArgs A) {
+    Ctl* ctl = A.ctl;
+    if (!(ctl->any & ANY_MAX)) return;
+    const int nwork = ctl->nwork;
+    const float arrive = ctl->arrive, deep = ctl->deep;
+    const int tid = threadIdx.x, jj = tid >> 5, ii = tid & 31;
+    for (int a = blockIdx.x; a < nwork; a += gridDim.x) {
+        const int t = A.list[a];
+        const int run = A.tile_run[t];
+        if ((A.R.flags[run] & (F_RUN | F_MAX)) != (F_RUN | F_MAX)) continue;
+        if ((A.bmark[t * TILE + jj] >> ii) & 1u) continue;
+        const int p = A.R.parity[run];
+        const int k = (A.tiles[2 * t] * TILE + GY + jj) * A.px + A.tiles[2 * t + 1] * TILE + GX + ii;
+        envelope_cell(A, t * TILE2 + tid, k, A.d[k], A.hh[1 - p][k], A.R.max_time[run], arrive, deep, A.uu[0][1 - p],
+                      A.uu[1][1 - p]);
+    }
 }
 
 // ------------------------------------------------------------------ boundary, tally, control (one CTA)
@@ -697,8 +713,8 @@ __global__ void boundary_kernel(StepArgs A, int control) {
             A.d[k] = fmax32(A.d[r] + A.bd0[m], 0.0f);
         }
         if ((flags & F_MAX) == F_MAX)
-            envelope(A, fid_of_native(A, k), k, A.d[k], h_next[k], R.max_time[run], ctl->arrive, ctl->deep,
-                     A.uu[0][n], A.uu[1][n]);
+            envelope_cell(A, fid_of_native(A, k), k, A.d[k], h_next[k], R.max_time[run], ctl->arrive, ctl->deep,
+                          A.uu[0][n], A.uu[1][n]);
     }
     if (!control) return;
     for (int m = gtid; m < A.ntally; m += gstride) {
@@ -791,7 +807,7 @@ __global__ void prestep_kernel(StepArgs A) {
         const int act = activate && ctl->adaptive;
         R.flags[r] = F_RUN | (refresh ? F_WAVE : 0) | (activate ? F_WET : 0) | (want_max ? F_MAX : 0) | (act ? F_ACT : 0);
         if (refresh) R.wave_bits[r] = 0u;
-        mine |= ANY_RUN | (refresh ? ANY_WAVE : 0u) | (act ? ANY_ACT : 0u);
+        mine |= ANY_RUN | (refresh ? ANY_WAVE : 0u) | (act ? ANY_ACT : 0u) | (want_max ? ANY_MAX : 0u);
     }
     if (mine) atomicOr(&any, mine);
     __syncthreads();
@@ -943,7 +959,7 @@ __global__ void __launch_bounds__(256) maxima_kernel(StepArgs A, float time, flo
             const int jj = threadIdx.y * 4 + c, ii = threadIdx.x;
             const int k = base + jj * A.px + ii;
             const int pc = A.R.parity[A.tile_run[t]];
-            envelope(A, t * TILE2 + jj * TILE + ii, k, A.d[k], A.hh[pc][k], time, arrive, deep, A.uu[0][pc], A.uu[1][pc]);
+            envelope_cell(A, t * TILE2 + jj * TILE + ii, k, A.d[k], A.hh[pc][k], time, arrive, deep, A.uu[0][pc], A.uu[1][pc]);
         }
     }
 }

@@ -473,10 +473,34 @@ constexpr int U_FLOATS = U_R + RING * RPAD;
 constexpr int UPDATE_SMEM = U_FLOATS * 4;           // 34,328 bytes
 constexpr int UPDATE_THREADS = 256;
 
+// The first entry at or after a, in steps of the grid, whose run is stepping (the same for every thread of a CTA).
+__device__ __forceinline__ int next_tile(const StepArgs& A, int a, int nwork) {
+    for (; a < nwork; a += gridDim.x)
+        if (A.R.flags[A.tile_run[A.list[a]]] & F_RUN) break;
+    return a;
+}
+
+// Issue (thread 0) the copies of tile t's update image against bar: the unscaled discharges and the old depth with
+// their ring, the residual, the source and Hc.
+__device__ __forceinline__ void update_issue(float* sm, uint64_t* bar, const TMaps& M, const StepArgs& A, int t) {
+    const int p = A.R.parity[A.tile_run[t]];
+    const int tj = A.tiles[2 * t], ti = A.tiles[2 * t + 1];
+    fence_proxy_async();
+    mbar_expect_tx(bar, (uint32_t)(3 * BOX + 3 * TILE2) * 4u);
+    const int x0 = ti * TILE + GX - 4, y0 = tj * TILE + GY - 2;
+    tma_load_2d(sm + U_QX1 * BOX, &M.qx1, x0, y0, bar);
+    tma_load_2d(sm + U_QY1 * BOX, &M.qy1, x0, y0, bar);
+    tma_load_2d(sm + U_H * BOX, &M.h[p], x0, y0, bar);
+    tma_load_2d(sm + U_OWN, &M.res, x0 + 4, y0 + 2, bar);
+    tma_load_2d(sm + U_OWN + TILE2, &M.src, x0 + 4, y0 + 2, bar);
+    bulk_load(sm + U_OWN + 2 * TILE2, A.hc + (size_t)t * TILE2, TILE2 * 4, bar);
+}
+
 // The update pass (wadi2d/solver/gpu/kernels/cells.cu:4-63 with limit fused in): TMA stages the tile's unscaled
 // discharges and old depth with their ring, its residual, source and Hc; r of the tile and its one-cell ring is
-// formed in shared memory; then each thread takes its four cells through continuity, issues their four level-table
-// loads together, and finishes the level, the wet share and the wet flag.
+// formed in shared memory; then each thread takes its four cells through continuity and issues their four
+// level-table loads together. Once every thread has read the image, thread 0 issues the next tile's copies into it,
+// and they land while the gathers return and the level, the wet share and the wet flag are finished.
 __global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_constant__ TMaps M, StepArgs A) {
     extern __shared__ __align__(128) float sm[];
     __shared__ __align__(8) uint64_t bar;
@@ -491,7 +515,6 @@ __global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_con
         fence_barrier_init();
     }
     __syncthreads();
-    const uint32_t bytes = (uint32_t)(3 * BOX + 3 * TILE2) * 4u;
     uint32_t phase = 0;
     const float* QX1 = sm + U_QX1 * BOX;
     const float* QY1 = sm + U_QY1 * BOX;
@@ -500,11 +523,12 @@ __global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_con
     const float* SRC = sm + U_OWN + TILE2;
     const float* HC = sm + U_OWN + 2 * TILE2;
     float* rs = sm + U_R;
-    for (int a = blockIdx.x; a < nwork; a += gridDim.x) {
+    int a = next_tile(A, blockIdx.x, nwork);
+    if (tid == 0 && a < nwork) update_issue(sm, &bar, M, A, A.list[a]);
+    while (a < nwork) {
         const int t = A.list[a];
         const int run = A.tile_run[t];
         const int flags = A.R.flags[run];
-        if (!(flags & F_RUN)) continue;  // uniform over the CTA
         const float dt = A.R.dtf[run];
         const float dxr = A.R.dx[run];
         const float area = dxr * dxr;
@@ -513,17 +537,6 @@ __global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_con
         const int p = A.R.parity[run];
         float* __restrict__ h_next = A.hh[1 - p];
         const int tj = A.tiles[2 * t], ti = A.tiles[2 * t + 1];
-        if (tid == 0) {
-            fence_proxy_async();
-            mbar_expect_tx(&bar, bytes);
-            const int x0 = ti * TILE + GX - 4, y0 = tj * TILE + GY - 2;
-            tma_load_2d(sm + U_QX1 * BOX, &M.qx1, x0, y0, &bar);
-            tma_load_2d(sm + U_QY1 * BOX, &M.qy1, x0, y0, &bar);
-            tma_load_2d(sm + U_H * BOX, &M.h[p], x0, y0, &bar);
-            tma_load_2d(sm + U_OWN, &M.res, x0 + 4, y0 + 2, &bar);
-            tma_load_2d(sm + U_OWN + TILE2, &M.src, x0 + 4, y0 + 2, &bar);
-            bulk_load(sm + U_OWN + 2 * TILE2, A.hc + (size_t)t * TILE2, TILE2 * 4, &bar);
-        }
         const bool ok = mbar_wait(&bar, phase);
         phase ^= 1u;
         if (__syncthreads_or(!ok)) {
@@ -544,7 +557,7 @@ __global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_con
         const int base = (tj * TILE + GY) * px + ti * TILE + GX;
         const float2* __restrict__ pairs_t = A.dtab2 + (size_t)t * (rows - 1) * TILE2;
         // continuity (cells.cu:219-232) for the thread's four cells
-        float hn[4], sv[4];
+        float hn[4], sv[4], hcs[4];
         int rr[4];
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
@@ -568,6 +581,7 @@ __global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_con
             h_next[k] = hn[c];
             // the level table's row (common.cuh cell_level): the top row above Hc, none where Hc <= 0
             const float hcv = HC[local];
+            hcs[c] = hcv;
             if (hcv <= 0.0f) {
                 rr[c] = -1;
                 sv[c] = 0.0f;
@@ -585,13 +599,16 @@ __global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_con
             const int local = (threadIdx.y * 4 + c) * TILE + threadIdx.x;
             pr[c] = rr[c] >= 0 ? __ldg(pairs_t + (size_t)rr[c] * TILE2 + local) : make_float2(0.0f, 0.0f);
         }
+        // every thread has read the image and r: the next tile's copies land in it during this tile's gathers
+        __syncthreads();
+        const int an = next_tile(A, a + gridDim.x, nwork);
+        if (tid == 0 && an < nwork) update_issue(sm, &bar, M, A, A.list[an]);
         int any = 0;
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const int jj = threadIdx.y * 4 + c, ii = threadIdx.x;
-            const int local = jj * TILE + ii;
             const int k = base + jj * px + ii;
-            const float hcv = HC[local];
+            const float hcv = hcs[c];
             const float h = hn[c];
             float dk, om = 1.0f;
             if (hcv <= 0.0f) {
@@ -617,9 +634,8 @@ __global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_con
         if (want_wet) {
             const int w = __syncthreads_or(any);
             if (tid == 0) A.wet[t] = w;
-        } else {
-            __syncthreads();
         }
+        a = an;
     }
 }
 

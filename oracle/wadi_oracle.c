@@ -29,19 +29,34 @@
 #define STRIDE2 (STRIDE * STRIDE)
 #define TILE2 (TILE * TILE)
 
+/* The step section's arithmetic type: float (the reference's arithmetic, bit for bit) or, compiled with
+ * -DOR_REAL_DOUBLE, double (the FP64 run that the float results are measured against; same statements, constants
+ * and table values, every operation in double). */
+#ifdef OR_REAL_DOUBLE
+typedef double real;
+#define R(x) x
+#define RSQRT sqrt
+#define RABS fabs
+#else
+typedef float real;
+#define R(x) x##f
+#define RSQRT sqrtf
+#define RABS fabsf
+#endif
+
 typedef struct {
-    float g, dx, e_wet, h_cfl, u_max, lead, a_min;
+    real g, dx, e_wet, h_cfl, u_max, lead, a_min;
     int32_t rows, second, sheet, mirror, carry;
 } OrParams;
 
 typedef struct {
-    float *h, *d, *u, *v, *mx, *my, *qx, *qy;
-    float *u1, *v1, *mx1, *my1, *qx1, *qy1, *r, *src, *res, *om;
-    const float *zcx, *zcy;
-    const float *Hc, *dtab;
-    const float *flx, *frx, *glx, *grx, *efx, *cwx, *ftabx;
-    const float *fly, *fry, *gly, *gry, *efy, *cwy, *ftaby;
-    float *wave;
+    real *h, *d, *u, *v, *mx, *my, *qx, *qy;
+    real *u1, *v1, *mx1, *my1, *qx1, *qy1, *r, *src, *res, *om;
+    const real *zcx, *zcy;
+    const real *Hc, *dtab;
+    const real *flx, *frx, *glx, *grx, *efx, *cwx, *ftabx;
+    const real *fly, *fry, *gly, *gry, *efy, *cwy, *ftaby;
+    real *wave;
     int32_t *wet;
 } OrArrays;
 
@@ -57,227 +72,227 @@ int or_threads(int n) {
 
 /* ------------------------------------------------------------------ float32 helpers (cpu/kernels.py:19-83) */
 
-static inline float cbrt32(float x) { return (float)cbrt((double)x); }
-static inline float fmax32(float a, float b) { return a >= b ? a : b; } /* Python max(a, b) on ordered values */
-static inline float fmin32(float a, float b) { return a <= b ? a : b; }
+static inline real cbrt32(real x) { return (real)cbrt((double)x); }
+static inline real fmax32(real a, real b) { return a >= b ? a : b; } /* Python max(a, b) on ordered values */
+static inline real fmin32(real a, real b) { return a <= b ? a : b; }
 
-static inline float minmod(float a, float b) {
-    if (a * b <= 0.0f) return 0.0f;
-    return fabsf(a) < fabsf(b) ? a : b;
+static inline real minmod(real a, real b) {
+    if (a * b <= R(0.0)) return R(0.0);
+    return RABS(a) < RABS(b) ? a : b;
 }
 
-static inline float ustar(float uc, float uup, float udown, int second) {
+static inline real ustar(real uc, real uup, real udown, int second) {
     if (!second) return uc;
-    return uc + 0.5f * minmod(uc - uup, udown - uc);
+    return uc + R(0.5) * minmod(uc - uup, udown - uc);
 }
 
-static inline float gated(float neighbour, float own, int mirror) {
-    return (mirror && neighbour == 0.0f) ? own : neighbour;
+static inline real gated(real neighbour, real own, int mirror) {
+    return (mirror && neighbour == R(0.0)) ? own : neighbour;
 }
 
 /* cell_level, cpu/kernels.py:39-48 */
-static inline float cell_level(float hb, float hc, const float *tab, int rows) {
-    if (hc <= 0.0f) return hb;
+static inline real cell_level(real hb, real hc, const real *tab, int rows) {
+    if (hc <= R(0.0)) return hb;
     int last = rows - 1;
     if (hb >= hc) return tab[last] + (hb - hc);
-    float s = sqrtf(hb / hc) * (float)last;
+    real s = RSQRT(hb / hc) * (real)last;
     int r = (int)s;
     if (r > last - 1) r = last - 1;
-    return tab[r] + (s - (float)r) * (tab[r + 1] - tab[r]);
+    return tab[r] + (s - (real)r) * (tab[r + 1] - tab[r]);
 }
 
 /* cell_plan, cpu/kernels.py:51-59 */
-static inline float cell_plan(float hb, float hc, const float *tab, int rows) {
-    if (hc <= 0.0f || hb >= hc) return 1.0f;
+static inline real cell_plan(real hb, real hc, const real *tab, int rows) {
+    if (hc <= R(0.0) || hb >= hc) return R(1.0);
     int last = rows - 1;
-    float s = sqrtf(hb / hc) * (float)last;
+    real s = RSQRT(hb / hc) * (real)last;
     int r = (int)s;
     if (r > last - 1) r = last - 1;
-    float m = (float)last;
-    return hc * (float)(2 * r + 1) / (m * m) / fmax32(tab[r + 1] - tab[r], 1e-12f);
+    real m = (real)last;
+    return hc * (real)(2 * r + 1) / (m * m) / fmax32(tab[r + 1] - tab[r], R(1e-12));
 }
 
 /* face_lookup, cpu/kernels.py:62-83 */
-static inline void face_lookup(float e, float top, const float *tab, int rows, float *A, float *T, float *W) {
+static inline void face_lookup(real e, real top, const real *tab, int rows, real *A, real *T, real *W) {
     int last = rows - 1;
-    float m = (float)last;
+    real m = (real)last;
     if (e >= top) {
-        float a1 = tab[2 * last];
-        float a0 = tab[2 * last - 2];
-        float c = (m - 1.0f) / m;
-        float w = (a1 - a0) / (top * (1.0f - c * c));
-        float area = a1 + w * (e - top);
+        real a1 = tab[2 * last];
+        real a0 = tab[2 * last - 2];
+        real c = (m - R(1.0)) / m;
+        real w = (a1 - a0) / (top * (R(1.0) - c * c));
+        real area = a1 + w * (e - top);
         *A = area;
-        *T = tab[2 * last + 1] * (area / fmax32(a1, 1e-12f));
+        *T = tab[2 * last + 1] * (area / fmax32(a1, R(1e-12)));
         *W = w;
         return;
     }
-    float s = sqrtf(e / top) * m;
+    real s = RSQRT(e / top) * m;
     int r = (int)s;
     if (r > last - 1) r = last - 1;
-    float c0 = (float)r / m;
-    float c1 = (float)(r + 1) / m;
-    float e0 = c0 * c0 * top;
-    float de = (c1 * c1 - c0 * c0) * top;
-    float f = (e - e0) / de;
-    float a0 = tab[2 * r];
-    float a1 = tab[2 * r + 2];
-    float t0 = tab[2 * r + 1];
+    real c0 = (real)r / m;
+    real c1 = (real)(r + 1) / m;
+    real e0 = c0 * c0 * top;
+    real de = (c1 * c1 - c0 * c0) * top;
+    real f = (e - e0) / de;
+    real a0 = tab[2 * r];
+    real a1 = tab[2 * r + 2];
+    real t0 = tab[2 * r + 1];
     *A = a0 + f * (a1 - a0);
     *T = t0 + f * (tab[2 * r + 3] - t0);
     *W = (a1 - a0) / de;
 }
 
 /* face_step, cpu/kernels.py:86-219. s: array step along the face normal, p: across it. Returns the wave speed. */
-static float face_step(int k, int fid, float dt, int want_wave, const OrParams *P, const float *om, const float *zc,
-                       int s, int p, const float *h, const float *d, const float *u, const float *m, const float *q,
-                       const float *qp, const float *vp, const float *fl, const float *fr, const float *gl,
-                       const float *gr, const float *ef, const float *cw, const float *ftab, float *u1, float *m1,
-                       float *q1) {
-    const float ZERO = 0.0f, HALF = 0.5f, ONE = 1.0f;
+static real face_step(int k, int fid, real dt, int want_wave, const OrParams *P, const real *om, const real *zc,
+                       int s, int p, const real *h, const real *d, const real *u, const real *m, const real *q,
+                       const real *qp, const real *vp, const real *fl, const real *fr, const real *gl,
+                       const real *gr, const real *ef, const real *cw, const real *ftab, real *u1, real *m1,
+                       real *q1) {
+    const real ZERO = R(0.0), HALF = R(0.5), ONE = R(1.0);
     const int rows = P->rows;
-    const float dx = P->dx;
-    const float span = dx;
-    float e_l = d[k - s] - fl[fid];
-    float e_r = d[k] - fr[fid];
-    float uf = u[k];
-    float e_lp = fmax32(e_l, ZERO);
-    float e_rp = fmax32(e_r, ZERO);
+    const real dx = P->dx;
+    const real span = dx;
+    real e_l = d[k - s] - fl[fid];
+    real e_r = d[k] - fr[fid];
+    real uf = u[k];
+    real e_lp = fmax32(e_l, ZERO);
+    real e_rp = fmax32(e_r, ZERO);
     int from_left = uf > ZERO || (uf == ZERO && e_l >= e_r);
-    float eup = from_left ? e_lp : e_rp;
+    real eup = from_left ? e_lp : e_rp;
     if (eup <= P->e_wet) {
         u1[k] = ZERO;
         m1[k] = ZERO;
         q1[k] = ZERO;
         return ZERO;
     }
-    float eface = eup;
+    real eface = eup;
     if (P->carry && cw[fid] == ZERO) {
-        float dz = from_left ? (zc[k - s] - fl[fid]) : (zc[k] - fr[fid]);
-        if (dz > 1e-6f) {
-            float phi = (eup - 2.0f * dz) / (2.0f * dz);
+        real dz = from_left ? (zc[k - s] - fl[fid]) : (zc[k] - fr[fid]);
+        if (dz > R(1e-6)) {
+            real phi = (eup - R(2.0) * dz) / (R(2.0) * dz);
             phi = phi < ZERO ? ZERO : (phi > ONE ? ONE : phi);
             eface = eup - phi * dz;
         }
     }
-    const float *tab = ftab + (size_t)2 * rows * fid;
-    float area, t, w;
+    const real *tab = ftab + (size_t)2 * rows * fid;
+    real area, t, w;
     face_lookup(eface, ef[fid], tab, rows, &area, &t, &w);
-    float h_l = h[k - s];
-    float h_r = h[k];
-    float hup = from_left ? h_l : h_r;
+    real h_l = h[k - s];
+    real h_r = h[k];
+    real hup = from_left ? h_l : h_r;
 
     /* [1] section */
-    float rho = ONE;
-    float d_eta = e_rp - e_lp;
+    real rho = ONE;
+    real d_eta = e_rp - e_lp;
     if (P->sheet) {
-        float avol = hup * dx;
-        float edown = from_left ? e_rp : e_lp;
+        real avol = hup * dx;
+        real edown = from_left ? e_rp : e_lp;
         if (avol < area) {
-            float sub = fmin32(e_lp, e_rp) / fmax32(e_lp, e_rp);
-            float sub2 = sub * sub;
-            float alpha = sub2 * sub2;
+            real sub = fmin32(e_lp, e_rp) / fmax32(e_lp, e_rp);
+            real sub2 = sub * sub;
+            real alpha = sub2 * sub2;
             rho = alpha + (ONE - alpha) * avol / area;
         }
         if (edown <= ZERO) {
             /* [2] disconnected */
-            float g_u = from_left ? gl[fid] : gr[fid];
-            float g_d = from_left ? gr[fid] : gl[fid];
-            float h_d = from_left ? h_r : h_l;
-            float drop = (hup - g_u) - fmax32(h_d - g_d, HALF * (g_u - g_d));
-            float level_drop = fabsf(e_l - e_r);
-            float drive = fmax32(eup, fmin32(drop, level_drop));
+            real g_u = from_left ? gl[fid] : gr[fid];
+            real g_d = from_left ? gr[fid] : gl[fid];
+            real h_d = from_left ? h_r : h_l;
+            real drop = (hup - g_u) - fmax32(h_d - g_d, HALF * (g_u - g_d));
+            real level_drop = RABS(e_l - e_r);
+            real drive = fmax32(eup, fmin32(drop, level_drop));
             d_eta = from_left ? -drive : drive;
         }
     }
 
     /* [3] momentum fluxes */
     const int mirror = P->mirror, second = P->second;
-    float um = gated(u[k - s], uf, mirror);
-    float up = gated(u[k + s], uf, mirror);
-    float umm = gated(u[k - 2 * s], um, mirror);
-    float upp = gated(u[k + 2 * s], up, mirror);
-    float qc_l = HALF * (q[k - s] + q[k]);
-    float qc_r = HALF * (q[k] + q[k + s]);
-    float s_l = qc_l > ZERO ? ustar(um, umm, uf, second) : ustar(uf, up, um, second);
-    float s_r = qc_r > ZERO ? ustar(uf, um, up, second) : ustar(up, upp, uf, second);
-    float flux = qc_r * s_r - qc_l * s_l;
-    float qy_s = HALF * (qp[k - s] + qp[k]);
-    float qy_n = HALF * (qp[k - s + p] + qp[k + p]);
-    float u_s = gated(u[k - p], uf, mirror);
-    float u_n = gated(u[k + p], uf, mirror);
-    float uss = gated(u[k - 2 * p], u_s, mirror);
-    float unn = gated(u[k + 2 * p], u_n, mirror);
-    float us_s = qy_s > ZERO ? ustar(u_s, uss, uf, second) : ustar(uf, u_n, u_s, second);
-    float us_n = qy_n > ZERO ? ustar(uf, u_s, u_n, second) : ustar(u_n, unn, uf, second);
+    real um = gated(u[k - s], uf, mirror);
+    real up = gated(u[k + s], uf, mirror);
+    real umm = gated(u[k - 2 * s], um, mirror);
+    real upp = gated(u[k + 2 * s], up, mirror);
+    real qc_l = HALF * (q[k - s] + q[k]);
+    real qc_r = HALF * (q[k] + q[k + s]);
+    real s_l = qc_l > ZERO ? ustar(um, umm, uf, second) : ustar(uf, up, um, second);
+    real s_r = qc_r > ZERO ? ustar(uf, um, up, second) : ustar(up, upp, uf, second);
+    real flux = qc_r * s_r - qc_l * s_l;
+    real qy_s = HALF * (qp[k - s] + qp[k]);
+    real qy_n = HALF * (qp[k - s + p] + qp[k + p]);
+    real u_s = gated(u[k - p], uf, mirror);
+    real u_n = gated(u[k + p], uf, mirror);
+    real uss = gated(u[k - 2 * p], u_s, mirror);
+    real unn = gated(u[k + 2 * p], u_n, mirror);
+    real us_s = qy_s > ZERO ? ustar(u_s, uss, uf, second) : ustar(uf, u_n, u_s, second);
+    real us_n = qy_n > ZERO ? ustar(uf, u_s, u_n, second) : ustar(u_n, unn, uf, second);
     flux += qy_n * us_n - qy_s * us_s;
 
     /* [4] momentum and pressure */
-    float abar = HALF * (h_l + h_r) * dx;
-    float press = dt * P->g * d_eta / span;
-    float us;
-    if (abar > 1e-6f * dx)
+    real abar = HALF * (h_l + h_r) * dx;
+    real press = dt * P->g * d_eta / span;
+    real us;
+    if (abar > R(1e-6) * dx)
         us = (m[k] - dt * flux / span) / abar - press;
     else
         us = uf - press;
 
     /* [5] friction */
-    float vb = 0.25f * (vp[k - s] + vp[k] + vp[k - s + p] + vp[k + p]);
-    float t3 = t * t * t * cbrt32(t);
-    float fric = area * area / fmax32(t3, 1e-30f);
-    if (rho < ONE) fric = fric / fmax32(rho * cbrt32(rho), 1e-12f);
-    float a = dt * P->g * fric;
-    float sp = sqrtf(us * us + vb * vb);
-    float un = 2.0f * us / (ONE + sqrtf(ONE + 4.0f * a * sp));
-    if (fabsf(un) > P->u_max) un = un > ZERO ? P->u_max : -P->u_max;
+    real vb = R(0.25) * (vp[k - s] + vp[k] + vp[k - s + p] + vp[k + p]);
+    real t3 = t * t * t * cbrt32(t);
+    real fric = area * area / fmax32(t3, R(1e-30));
+    if (rho < ONE) fric = fric / fmax32(rho * cbrt32(rho), R(1e-12));
+    real a = dt * P->g * fric;
+    real sp = RSQRT(us * us + vb * vb);
+    real un = R(2.0) * us / (ONE + RSQRT(ONE + R(4.0) * a * sp));
+    if (RABS(un) > P->u_max) un = un > ZERO ? P->u_max : -P->u_max;
 
     /* [6] crest face */
-    float qn = area * rho * un;
-    float c = cw[fid];
+    real qn = area * rho * un;
+    real c = cw[fid];
     if (c != ZERO) {
-        float area_c = area, w_c = w;
+        real area_c = area, w_c = w;
         if (c < ZERO) {
             c = -c;
-            float ua = from_left ? um : up;
-            float tc;
+            real ua = from_left ? um : up;
+            real tc;
             face_lookup(eup + HALF * ua * ua / P->g, ef[fid], tab, rows, &area_c, &tc, &w_c);
         }
-        float qc = c * area_c * sqrtf(area_c / fmax32(w_c, 1e-9f));
-        if (fabsf(qn) > qc) {
+        real qc = c * area_c * RSQRT(area_c / fmax32(w_c, R(1e-9)));
+        if (RABS(qn) > qc) {
             qn = qn > ZERO ? qc : -qc;
-            un = qn / fmax32(area * rho, 1e-12f);
+            un = qn / fmax32(area * rho, R(1e-12));
         }
     }
     u1[k] = un;
     m1[k] = abar * un;
     q1[k] = qn;
     if (!want_wave) return ZERO;
-    if (!isfinite(un)) return 1e30f;
-    float d_left = d[k - s];
-    float d_right = d[k];
-    float dup = from_left ? d_left : d_right;
+    if (!isfinite(un)) return R(1e30);
+    real d_left = d[k - s];
+    real d_right = d[k];
+    real dup = from_left ? d_left : d_right;
     if (dup <= P->h_cfl) return ZERO;
-    float plan = from_left ? om[k - s] : om[k];
-    float dother = from_left ? d_right : d_left;
+    real plan = from_left ? om[k - s] : om[k];
+    real dother = from_left ? d_right : d_left;
     if (dother > P->h_cfl) plan = fmin32(plan, from_left ? om[k] : om[k - s]);
-    float wave = sqrtf(fmax32(P->g * area * rho / (fmax32(plan, P->a_min) * dx), ZERO));
-    return fabsf(un) + fmin32(P->lead * fabsf(un - uf), 2.0f * wave) + wave;
+    real wave = RSQRT(fmax32(P->g * area * rho / (fmax32(plan, P->a_min) * dx), ZERO));
+    return RABS(un) + fmin32(P->lead * RABS(un - uf), R(2.0) * wave) + wave;
 }
 
 /* faces, cpu/kernels.py:222-244 */
-void or_faces(const OrArrays *A, const OrParams *P, const int32_t *active, int nact, float dt, int want_wave) {
+void or_faces(const OrArrays *A, const OrParams *P, const int32_t *active, int nact, real dt, int want_wave) {
 #pragma omp parallel for schedule(dynamic, 4)
     for (int a = 0; a < nact; ++a) {
         int t = active[a];
-        float w = 0.0f;
+        real w = R(0.0);
         for (int j = 0; j < TILE; ++j) {
             for (int i = 0; i < TILE; ++i) {
                 int k = t * STRIDE2 + (j + HALO) * STRIDE + i + HALO;
                 int fid = t * TILE2 + j * TILE + i;
-                float wx = face_step(k, fid, dt, want_wave, P, A->om, A->zcx, 1, STRIDE, A->h, A->d, A->u, A->mx, A->qx,
+                real wx = face_step(k, fid, dt, want_wave, P, A->om, A->zcx, 1, STRIDE, A->h, A->d, A->u, A->mx, A->qx,
                                      A->qy, A->v, A->flx, A->frx, A->glx, A->grx, A->efx, A->cwx, A->ftabx, A->u1, A->mx1,
                                      A->qx1);
-                float wy = face_step(k, fid, dt, want_wave, P, A->om, A->zcy, STRIDE, 1, A->h, A->d, A->v, A->my, A->qy,
+                real wy = face_step(k, fid, dt, want_wave, P, A->om, A->zcy, STRIDE, 1, A->h, A->d, A->v, A->my, A->qy,
                                      A->qx, A->u, A->fly, A->fry, A->gly, A->gry, A->efy, A->cwy, A->ftaby, A->v1, A->my1,
                                      A->qy1);
                 w = fmax32(w, fmax32(wx, wy));
@@ -288,31 +303,31 @@ void or_faces(const OrArrays *A, const OrParams *P, const int32_t *active, int n
 }
 
 /* limit, cpu/kernels.py:247-262 */
-void or_limit(const OrArrays *A, const OrParams *P, const int32_t *active, int nact, float dt) {
-    const float dx = P->dx;
-    const float area = dx * dx;
+void or_limit(const OrArrays *A, const OrParams *P, const int32_t *active, int nact, real dt) {
+    const real dx = P->dx;
+    const real area = dx * dx;
 #pragma omp parallel for schedule(static)
     for (int a = 0; a < nact; ++a) {
         int t = active[a];
         for (int j = 0; j < TILE; ++j) {
             for (int i = 0; i < TILE; ++i) {
                 int k = t * STRIDE2 + (j + HALO) * STRIDE + i + HALO;
-                float out = fmax32(A->qx1[k + 1], 0.0f) + fmax32(-A->qx1[k], 0.0f) + fmax32(A->qy1[k + STRIDE], 0.0f) +
-                            fmax32(-A->qy1[k], 0.0f);
-                float have = fmax32(A->h[k], 0.0f) * area;
-                A->r[k] = out * dt > have ? have / (out * dt) : 1.0f;
+                real out = fmax32(A->qx1[k + 1], R(0.0)) + fmax32(-A->qx1[k], R(0.0)) + fmax32(A->qy1[k + STRIDE], R(0.0)) +
+                            fmax32(-A->qy1[k], R(0.0));
+                real have = fmax32(A->h[k], R(0.0)) * area;
+                A->r[k] = out * dt > have ? have / (out * dt) : R(1.0);
             }
         }
     }
 }
 
-static inline float scaled(float q, float rl, float rr) { return q * (q > 0.0f ? rl : rr); }
+static inline real scaled(real q, real rl, real rr) { return q * (q > R(0.0) ? rl : rr); }
 
 /* update, cpu/kernels.py:270-299 (debt = False on the uniform step) */
-void or_update(const OrArrays *A, const OrParams *P, const int32_t *active, int nact, float dt, int want_plan) {
+void or_update(const OrArrays *A, const OrParams *P, const int32_t *active, int nact, real dt, int want_plan) {
     const int rows = P->rows;
-    const float dx = P->dx;
-    const float area = dx * dx;
+    const real dx = P->dx;
+    const real area = dx * dx;
 #pragma omp parallel for schedule(static)
     for (int a = 0; a < nact; ++a) {
         int t = active[a];
@@ -321,24 +336,24 @@ void or_update(const OrArrays *A, const OrParams *P, const int32_t *active, int 
             for (int i = 0; i < TILE; ++i) {
                 int k = t * STRIDE2 + (j + HALO) * STRIDE + i + HALO;
                 int fid = t * TILE2 + j * TILE + i;
-                const float *r = A->r;
-                float rc = r[k];
-                float qw = scaled(A->qx1[k], r[k - 1], rc);
-                float qe = scaled(A->qx1[k + 1], rc, r[k + 1]);
-                float qn = scaled(A->qy1[k], r[k - STRIDE], rc);
-                float qs = scaled(A->qy1[k + STRIDE], rc, r[k + STRIDE]);
+                const real *r = A->r;
+                real rc = r[k];
+                real qw = scaled(A->qx1[k], r[k - 1], rc);
+                real qe = scaled(A->qx1[k + 1], rc, r[k + 1]);
+                real qn = scaled(A->qy1[k], r[k - STRIDE], rc);
+                real qs = scaled(A->qy1[k + STRIDE], rc, r[k + STRIDE]);
                 A->qx[k] = qw;
                 A->qy[k] = qn;
-                float h0 = A->h[k];
-                float inc = A->res[k] + dt * A->src[k] - dt * (qe - qw + qs - qn) / area;
-                float total = h0 + inc;
-                float hn = fmax32(total, 0.0f);
-                A->res[k] = total > 0.0f ? inc - (total - h0) : 0.0f;
+                real h0 = A->h[k];
+                real inc = A->res[k] + dt * A->src[k] - dt * (qe - qw + qs - qn) / area;
+                real total = h0 + inc;
+                real hn = fmax32(total, R(0.0));
+                A->res[k] = total > R(0.0) ? inc - (total - h0) : R(0.0);
                 A->h[k] = hn;
-                const float *tab = A->dtab + (size_t)rows * fid;
+                const real *tab = A->dtab + (size_t)rows * fid;
                 A->d[k] = cell_level(hn, A->Hc[fid], tab, rows);
                 if (want_plan) A->om[k] = cell_plan(hn, A->Hc[fid], tab, rows);
-                if (hn > 0.0f) any_wet = 1;
+                if (hn > R(0.0)) any_wet = 1;
             }
         }
         A->wet[t] = any_wet;
@@ -361,7 +376,7 @@ void or_plan(const OrArrays *A, const OrParams *P, const int32_t *tiles, int n) 
 }
 
 /* exchange, cpu/kernels.py:314-319 */
-void or_exchange(const int32_t *active, int nact, const int32_t *slot, const int32_t *src, int nhalo, float *a) {
+void or_exchange(const int32_t *active, int nact, const int32_t *slot, const int32_t *src, int nhalo, real *a) {
 #pragma omp parallel for schedule(static)
     for (int n = 0; n < nact; ++n) {
         int t = active[n];
@@ -370,34 +385,34 @@ void or_exchange(const int32_t *active, int nact, const int32_t *slot, const int
 }
 
 /* boundary, cpu/kernels.py:322-334 (sequential: a follow cell reads its reference after earlier ones are set) */
-void or_boundary(int n, const int32_t *cell, const int32_t *ref, const int32_t *kind, const float *d0, const float *h0,
-                 float *h, float *d) {
+void or_boundary(int n, const int32_t *cell, const int32_t *ref, const int32_t *kind, const real *d0, const real *h0,
+                 real *h, real *d) {
     for (int m = 0; m < n; ++m) {
         int k = cell[m];
         if (kind[m] == 0) {
             h[k] = h0[m];
             d[k] = d0[m];
         } else if (kind[m] == 1) {
-            h[k] = 0.0f;
-            d[k] = 0.0f;
+            h[k] = R(0.0);
+            d[k] = R(0.0);
         } else {
             h[k] = h[ref[m]];
-            d[k] = fmax32(d[ref[m]] + d0[m], 0.0f);
+            d[k] = fmax32(d[ref[m]] + d0[m], R(0.0));
         }
     }
 }
 
 /* maxima, engine/maxima.py:75-92. The literal 0.5 is a float64, so the centre speed is formed in float64 and each
  * envelope entry takes the float32 rounding of its new maximum. */
-void or_maxima(const int32_t *active, int nact, float time, float arrive, float deep, const float *d, const float *h,
-               const float *u, const float *v, float *dmax, float *hmax, float *smax, float *zmax, float *tarr) {
+void or_maxima(const int32_t *active, int nact, real time, real arrive, real deep, const real *d, const real *h,
+               const real *u, const real *v, real *dmax, real *hmax, real *smax, real *zmax, real *tarr) {
 #pragma omp parallel for schedule(static)
     for (int a = 0; a < nact; ++a) {
         int t = active[a];
         for (int j = 0; j < TILE; ++j)
             for (int i = 0; i < TILE; ++i) {
                 int k = t * STRIDE2 + (j + HALO) * STRIDE + i + HALO;
-                float dk = d[k];
+                real dk = d[k];
                 dmax[k] = fmax32(dmax[k], dk);
                 hmax[k] = fmax32(hmax[k], h[k]);
                 if (dk > deep) {
@@ -405,21 +420,21 @@ void or_maxima(const int32_t *active, int nact, float time, float arrive, float 
                     double vc = 0.5 * (double)(v[k] + v[k + STRIDE]);
                     double s = sqrt(uc * uc + vc * vc);
                     double sm = (double)smax[k];
-                    smax[k] = (float)(sm >= s ? sm : s);
+                    smax[k] = (real)(sm >= s ? sm : s);
                     double hz = s * (double)dk;
                     double zm = (double)zmax[k];
-                    zmax[k] = (float)(zm >= hz ? zm : hz);
+                    zmax[k] = (real)(zm >= hz ? zm : hz);
                 }
-                if (tarr[k] < 0.0f && dk >= arrive) tarr[k] = time;
+                if (tarr[k] < R(0.0) && dk >= arrive) tarr[k] = time;
             }
     }
 }
 
 /* tally, engine/maxima.py:95-100 and :171-182 (the device form: one FP64 total per face, dt * sign * q) */
-void or_tally(int n, double dt, const int32_t *face, const int32_t *axis, const float *sign, const float *qx,
-              const float *qy, double *total) {
+void or_tally(int n, double dt, const int32_t *face, const int32_t *axis, const real *sign, const real *qx,
+              const real *qy, double *total) {
     for (int m = 0; m < n; ++m) {
-        float q = axis[m] ? qy[face[m]] : qx[face[m]];
+        real q = axis[m] ? qy[face[m]] : qx[face[m]];
         total[m] += dt * (double)(sign[m] * q);
     }
 }

@@ -26,10 +26,12 @@ class OracleApi:
         return O.Boundary(cell, ref, kind, d0, h0)
 
     def maxima(self, m, arrive, deep):
-        return O.Maxima(m, arrive, deep)
+        self._maxima = O.Maxima(m, arrive, deep)
+        return self._maxima
 
     def tally(self, m, xf, xs, yf, ys):
-        return O.Tally(m, xf, xs, yf, ys)
+        self._tally = O.Tally(m, xf, xs, yf, ys)
+        return self._tally
 
     def hbar_at_level(self, level, zmin, hc, dtab):
         return O.hbar_at_level(level, zmin, hc, dtab)
@@ -42,3 +44,33 @@ class OracleApi:
 
     def crest(self, shape):
         return O.Crest.empty(shape)
+
+
+class Fp64Api(OracleApi):
+    """The FP64 run (oracle/fp64.py) through the same calls, stepped through a given dt sequence: ``advance`` replays
+    ``dts`` (a float32 run's own steps) instead of applying the dt rule."""
+
+    def __init__(self, dts) -> None:
+        super().__init__()
+        self._replay = [float(x) for x in dts]
+
+    def model(self, grid, tables, numerics):
+        from oracle import fp64
+
+        m = fp64.Model64(grid, tables, O.Numerics(**numerics))
+        replay = self._replay
+        m.advance = lambda t_end, on_step=None: m.replay(replay, on_step)
+        self.dts = m.dts
+        return m
+
+    def maxima(self, m, arrive, deep):
+        from oracle import fp64
+
+        self._maxima = fp64.Maxima64(m, arrive, deep)
+        return self._maxima
+
+    def tally(self, m, xf, xs, yf, ys):
+        from oracle import fp64
+
+        self._tally = fp64.Tally64(m, xf, xs, yf, ys)
+        return self._tally

@@ -529,7 +529,13 @@ int32_t w2b_build_tables(const W2BTableIn* in, const W2BTableOut* out, void* str
                     cudaGetErrorString(cudaGetLastError()));
             return W2B_ECUDA;
         }
-        face_tables_kernel<true><<<sms, threads, bytes, s>>>(A);
+        // as many CTAs a SM as their workspaces allow: short face lines leave room for several
+        int occ = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, face_tables_kernel<true>, threads, bytes) !=
+                cudaSuccess ||
+            occ < 1)
+            occ = 1;
+        face_tables_kernel<true><<<sms * occ, threads, bytes, s>>>(A);
     } else {
         const int64_t fthreads = in->local ? out->ws_threads : (int64_t)148 * 8 * 128;
         face_tables_kernel<false><<<(unsigned)(fthreads / 128), 128, 0, s>>>(A);

@@ -65,6 +65,10 @@ def parse():
     p.add_argument("--recession-min", type=float, default=30.0, help="simulated time after each storm, minutes")
     p.add_argument("--time-scale", type=float, default=1.0, help="share of each run's simulated time to step")
     p.add_argument("--skip-plain", action="store_true", help="the batch only (no one-after-another sweep)")
+    p.add_argument("--arf-study", action="store_true",
+                   help="the depth-area (ARF) study: every storm area of one catchment as one batch, against one run "
+                        "after another")
+    p.add_argument("--study-n", type=int, default=1024, help="--arf-study: catchment cells a side")
     p.add_argument("--config2-run", action="store_true",
                    help="configuration 2 end to end: 1024 x 1024, crests, lumped inflows, a reservoir, 6 h")
     p.add_argument("--table-build", action="store_true",
@@ -643,6 +647,50 @@ def table_build(args) -> None:
     print(json.dumps({"run": "GPU table build", **out}), flush=True)
 
 
+def arf_study(args) -> None:
+    """The depth-area study (the reference's ``wadi2d arf``): configuration 5's catchment (a seeded fractal fan at
+    10 m with 4 x 4 pixels, 8 design lines on its channels), storm areas bracketing the lines' D8 drainage areas
+    (ratio 2, at most 8), a uniform 60 mm storm over 2 h read through an area-reduction table, 3 h from dry ground;
+    all storm areas as one batch against one run after another, CUDA-event time around the runs."""
+    import torch
+
+    from wadi2d_b200 import critical as C
+    from wadi2d_b200 import study as S
+    from wadi2d_b200.forcing import ArfTable, UniformStorm
+
+    t0 = time.perf_counter()
+    cat = C.prepare(n=args.study_n, dx=10.0, k=4, seed=17)
+    areas, cell, line_a = S.bracketing_areas(cat, ratio=2.0, most=8)
+    torch.cuda.synchronize()
+    setup = time.perf_counter() - t0
+    arf = ArfTable(np.array([0.1, 1.0, 10.0, 100.0, 1000.0]), np.array([1.0, 0.95, 0.86, 0.72, 0.55]))
+    storm = UniformStorm(60.0, 120.0, arf=arf)
+    names = [f"line{n}" for n in range(len(cat.lines))]
+    kw = dict(t_end=3 * 3600.0, window=30.0, every=4, kind="storm-centred")
+    b = S.run_study(cat, storm, areas, names, list(line_a), cell, batched=True, **kw)
+    p = S.run_study(cat, storm, areas, names, list(line_a), cell, batched=False, **kw)
+    cells = int(cat.grid.mask.sum())
+    n = len(areas)
+    line = {
+        "run": "ARF depth-area study", "cells": cells, "storm_areas_km2": [round(a, 4) for a in areas],
+        "lines": len(cat.lines), "setup_s": setup,
+        "batch": {"s": b.seconds, "runs_per_h": 3600.0 * n / b.seconds,
+                  "cell_steps_per_s": float(cells * b.steps.sum() / b.seconds)},
+        "plain": {"s": p.seconds, "runs_per_h": 3600.0 * n / p.seconds,
+                  "cell_steps_per_s": float(cells * p.steps.sum() / p.seconds)},
+        "speedup": p.seconds / b.seconds,
+        "same_steps": bool(np.array_equal(b.steps, p.steps)),
+        "same_table": b.table == p.table,
+        "same_composites": all(np.array_equal(b.composite[k], p.composite[k]) for k in S.COMPOSITE_MAPS),
+        "steps": [int(x) for x in b.steps],
+        "table": [{k: (round(v, 4) if isinstance(v, float) else v) for k, v in r.items()
+                   if k in ("design_point", "drainage_area_km2", "design_peak_m3s", "time_of_peak_s")}
+                  for r in b.table],
+        "composite_max": {k: float(v.max()) for k, v in b.composite.items()},
+    }  # fmt: skip
+    print(json.dumps(line), flush=True)
+
+
 def main() -> None:
     args = parse()
     if args.impl == "reference":
@@ -662,6 +710,9 @@ def main() -> None:
         return
     if args.config2_run:
         config2_run(args)
+        return
+    if args.arf_study:
+        arf_study(args)
         return
     import torch
     import torch.distributed as dist

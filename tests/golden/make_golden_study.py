@@ -1,0 +1,92 @@
+"""Make the golden vectors of the depth-area study's host arithmetic: run the reference's own functions on seeded
+inputs.
+
+Run in a container that holds the reference source tree (read-only is fine):
+
+    WADI2D_REFERENCE=/root/reference python tests/golden/make_golden_study.py
+
+The reference's study module (wadi2d/arf.py) imports its I/O stack (rasterio, h5py and the products) at the top, which
+this image does not have, so the script reads the module's source, takes the definitions of its pure numpy helpers
+(``bracket_areas``, ``run_name``, ``interpolate_peak``, ``_row``, ``interpolated_row``, ``log_area_weights``,
+``composite_map``) and executes those alone, with numpy. It writes ``study.npz`` (inputs and outputs) and
+``study.json`` (the interpolated design rows and the run names). Nothing on the GPU side reads the reference.
+"""
+
+from __future__ import annotations
+
+import ast
+import json
+import os
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+REF = Path(os.environ.get("WADI2D_REFERENCE", "/root/reference"))
+WANTED = ("bracket_areas", "run_name", "interpolate_peak", "_row", "interpolated_row", "log_area_weights",
+          "composite_map")  # fmt: skip
+
+
+def reference_helpers() -> dict:
+    src = (REF / "wadi2d" / "arf.py").read_text()
+    tree = ast.parse(src)
+    keep = [node for node in tree.body if isinstance(node, ast.FunctionDef) and node.name in WANTED]
+    missing = set(WANTED) - {node.name for node in keep}
+    if missing:
+        raise SystemExit(f"not found in wadi2d/arf.py: {sorted(missing)}")
+    module = ast.Module(body=keep, type_ignores=[])
+    ns: dict = {"np": np, "__name__": "reference_arf_helpers"}
+    exec(compile(module, str(REF / "wadi2d" / "arf.py"), "exec"), ns)  # noqa: S102 - the reference's own helpers
+    return ns
+
+
+def main() -> None:
+    R = reference_helpers()
+    rng = np.random.default_rng(31)
+    out: dict[str, np.ndarray] = {}
+    meta: dict[str, object] = {}
+
+    # bracket_areas: (wanted, ratio, most)
+    bracket_cases = [
+        ([3.0, 40.0, 12.5], 2.0, 8),
+        ([5.0, 5.0], 2.0, 8),
+        ([1.0, 1000.0], 1.5, 6),
+        ([0.7, 2.1], 3.0, 10),
+        ([12.0, 13.0, 250.0, 90.0], 1.8, 12),
+    ]
+    meta["bracket"] = [
+        {"wanted": w, "ratio": r, "most": m, "areas": [float(x) for x in R["bracket_areas"](w, r, m)]}
+        for w, r, m in bracket_cases
+    ]
+    meta["run_names"] = {str(a): R["run_name"](a) for a in (0.5, 12.25, 1234.5678, 10.0)}
+
+    # interpolate_peak and interpolated_row
+    areas = np.geomspace(1.0, 300.0, 7)
+    peaks = rng.uniform(5.0, 500.0, 7)
+    peaks[2] = 0.0  # a dry run
+    times = rng.uniform(1800.0, 20000.0, 7)
+    queries = np.array([0.5, 1.0, 2.2, 5.0, 17.0, 80.0, 300.0, 900.0])
+    out["ip_areas"], out["ip_peaks"], out["ip_times"], out["ip_queries"] = areas, peaks, times, queries
+    out["ip_result"] = np.array([R["interpolate_peak"](areas, peaks, float(q)) for q in queries])
+    out["ip_dry"] = np.array([R["interpolate_peak"](areas, np.zeros(7), 3.0)])
+    meta["rows"] = [
+        R["interpolated_row"](f"P{n}", float(q), areas, peaks, times, "storm-centred", "design line, 2D runs either side")
+        for n, q in enumerate(queries)
+    ]
+
+    # log_area_weights and composite_map
+    cell_area = np.exp(rng.uniform(np.log(0.3), np.log(600.0), (24, 32)))
+    low, high, w = R["log_area_weights"](areas, cell_area)
+    out["lw_cell_area"], out["lw_low"], out["lw_high"], out["lw_w"] = cell_area, low, high, w
+    maps = [rng.uniform(0.0, 3.0, (24, 32)) for _ in range(areas.size)]
+    out["cm_maps"] = np.stack(maps)
+    out["cm_result"] = R["composite_map"](maps, areas, cell_area)
+    out["cm_single"] = R["composite_map"](maps[:1], areas[:1], cell_area)
+
+    np.savez_compressed(HERE / "study.npz", **out)
+    (HERE / "study.json").write_text(json.dumps(meta, indent=1))
+    print("wrote study.npz, study.json")
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,73 @@
+"""The depth-area study's readings against the reference's own functions (tests/golden/make_golden_study.py ran
+wadi2d/arf.py's helpers on these inputs): storm areas, run names, interpolated peaks and design rows, log-area weights
+and composite maps."""
+
+from __future__ import annotations
+
+import json
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+from wadi2d_b200 import study as S
+
+GOLD = Path(__file__).resolve().parent / "golden"
+
+
+@pytest.fixture(scope="module")
+def gold():
+    return np.load(GOLD / "study.npz"), json.loads((GOLD / "study.json").read_text())
+
+
+def test_bracket_areas_and_run_names(gold):
+    _, meta = gold
+    for case in meta["bracket"]:
+        assert S.bracket_areas(case["wanted"], case["ratio"], case["most"]) == case["areas"]
+    for area, name in meta["run_names"].items():
+        assert S.run_name(float(area)) == name
+
+
+def test_interpolated_peaks_and_rows(gold):
+    g, meta = gold
+    got = np.array([S.interpolate_peak(g["ip_areas"], g["ip_peaks"], float(q)) for q in g["ip_queries"]])
+    assert np.array_equal(got, g["ip_result"])
+    assert S.interpolate_peak(g["ip_areas"], np.zeros(7), 3.0) == float(g["ip_dry"][0])
+    for n, (q, row) in enumerate(zip(g["ip_queries"], meta["rows"], strict=True)):
+        mine = S.interpolated_row(f"P{n}", float(q), g["ip_areas"], g["ip_peaks"], g["ip_times"], "storm-centred",
+                                  S.READ_LINE)  # fmt: skip
+        assert mine == row
+        assert list(mine) == list(row)  # the CSV's column order
+
+
+def test_design_table_reads_each_line(gold):
+    g, meta = gold
+    peaks = np.stack([g["ip_peaks"], g["ip_peaks"] * 7.0, g["ip_peaks"] * 2.0], axis=1)  # a column a line
+    times = np.stack([g["ip_times"]] * 3, axis=1)
+    rows = S.design_table(["P2", "skip", "P2b"], [2.2, None, 2.2], g["ip_areas"], peaks, times, "storm-centred")
+    assert [r["design_point"] for r in rows] == ["P2", "P2b"]
+    assert rows[0] == meta["rows"][2]
+    assert rows[1]["design_peak_m3s"] == pytest.approx(2.0 * rows[0]["design_peak_m3s"], rel=1e-12)
+
+
+def test_log_area_weights_and_composites(gold):
+    g, _ = gold
+    low, high, w = S.log_area_weights(g["ip_areas"], g["lw_cell_area"])
+    assert np.array_equal(low, g["lw_low"]) and np.array_equal(high, g["lw_high"])
+    assert np.array_equal(w, g["lw_w"])
+    maps = list(g["cm_maps"])
+    assert np.array_equal(S.composite_map(maps, g["ip_areas"], g["lw_cell_area"]), g["cm_result"])
+    assert np.array_equal(S.composite_map(maps[:1], g["ip_areas"][:1], g["lw_cell_area"]), g["cm_single"])
+
+
+def test_composites_from_envelopes_with_a_depth_floor():
+    rng = np.random.default_rng(2)
+    envs = [{k: rng.uniform(0.0, 1.0, (4, 5)) for k in ("depth", "speed", "hazard")} for _ in range(3)]
+    areas = [1.0, 4.0, 16.0]
+    cell = np.full((4, 5), 2.0)
+    out = S.composite_maps(envs, areas, cell, depth_floor=0.5)
+    w = np.log(2.0) / np.log(4.0)
+    for name, field in S.ENVELOPE_OF_MAP.items():
+        a = np.where(envs[0]["depth"] < 0.5, 0.0, envs[0][field])
+        b = np.where(envs[1]["depth"] < 0.5, 0.0, envs[1][field])
+        assert np.allclose(out[name], (1 - w) * a + w * b, rtol=0, atol=1e-15)

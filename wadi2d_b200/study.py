@@ -1,0 +1,243 @@
+"""The depth-area (ARF) study on the batch engine: one run per storm area, all of them advanced together.
+
+The reference runs a study's storm areas one after another through ``run_job`` (wadi2d/arf.py:346-372, ``_study``)
+and then reads them: each design line's peak between the two runs that bracket its drainage area, ln Q linear in
+ln A (``design_table``, arf.py:157-168), and per cell the same reading of the runs' max-depth, max-speed and hazard
+maps against an accumulation raster (``composite_maps``, arf.py:300-316). Here the runs share one grid and one set
+of device tables and go into one ``Batch``: each run is the same storm with its storm area set to one of the study's
+areas (the ARF table read there), its own clock, envelope and design lines, and each run steps exactly as it would
+alone. The readings below keep the reference's names, arguments and results (pinned by ``tests/test_study.py``
+against the reference's own functions); the job file, GeoTIFF and progress-file plumbing around them is the
+reference's run driver and stays there.
+"""
+
+from __future__ import annotations
+
+import dataclasses
+from dataclasses import dataclass, field
+
+import numpy as np
+
+COMPOSITE_MAPS = ("max_depth", "max_speed", "hazard")
+ENVELOPE_OF_MAP = {"max_depth": "depth", "max_speed": "speed", "hazard": "hazard"}
+"""Each composite's per-run map and the envelope field it is (wadi2d/products/cell_maps.py:79-89)."""
+READ_LINE = "design line, 2D runs either side"
+
+
+# ------------------------------------------------------------------------------------------------ storm areas
+
+
+def bracket_areas(wanted, ratio: float, most: int) -> list[float]:
+    """Storm areas spanning the wanted ones (wadi2d/arf.py:79-86): log-spaced from the smallest to the largest, as
+    few as keep neighbours within ``ratio`` of each other but at least two and at most ``most``; a single area when
+    the wanted areas are all the same."""
+    lo, hi = float(min(wanted)), float(max(wanted))
+    if hi <= lo * (1.0 + 1e-9):
+        return [lo]
+    gaps = int(np.ceil(np.log(hi / lo) / np.log(ratio) - 1e-9))
+    return list(np.geomspace(lo, hi, min(max(gaps + 1, 2), most)))
+
+
+def run_name(area: float) -> str:
+    """A run folder's name for a storm area (wadi2d/arf.py:118-119): km2 with three decimals, the point as 'p'."""
+    return ("A%010.3fkm2" % area).replace(".", "p")
+
+
+# ------------------------------------------------------------------------------------------------ readings
+
+
+def interpolate_peak(areas, peaks, area: float) -> float:
+    """A peak at drainage area ``area`` from the runs' peaks (wadi2d/arf.py:122-128): ln Q linear in ln A over the
+    runs that carried water, the end values held beyond them; 0 when no run did."""
+    areas, peaks = np.asarray(areas, np.float64), np.asarray(peaks, np.float64)
+    wet = peaks > 0.0
+    if not np.any(wet):
+        return 0.0
+    return float(np.exp(np.interp(np.log(area), np.log(areas[wet]), np.log(peaks[wet]))))
+
+
+def _design_row(name, area, a_low, a_high, q_low, q_high, q, t, kind, read_as) -> dict[str, object]:
+    """One row of design_points.csv, in the reference's column order (wadi2d/arf.py:131-143)."""
+    return {
+        "design_point": name,
+        "drainage_area_km2": area,
+        "storm_area_low_km2": float(a_low),
+        "storm_area_high_km2": float(a_high),
+        "peak_low_m3s": float(q_low),
+        "peak_high_m3s": float(q_high),
+        "design_peak_m3s": float(q),
+        "time_of_peak_s": float(t),
+        "arf_table_type": kind,
+        "read_as": read_as,
+    }
+
+
+def interpolated_row(name: str, area: float, grid_a, peaks, times, kind: str, read_as: str) -> dict[str, object]:
+    """The row of a point at drainage area ``area`` read from the runs either side of it (wadi2d/arf.py:145-154);
+    the time of the peak is the run nearer in ln A."""
+    grid_a = np.asarray(grid_a, np.float64)
+    peaks, times = np.asarray(peaks, np.float64), np.asarray(times, np.float64)
+    last = grid_a.size - 1
+    hi = min(max(int(np.searchsorted(grid_a, area)), 0), last)
+    lo = max(hi - 1, 0)
+    near = lo if abs(np.log(area / grid_a[lo])) <= abs(np.log(area / grid_a[hi])) else hi
+    q = interpolate_peak(grid_a, peaks, area)
+    return _design_row(name, area, grid_a[lo], grid_a[hi], peaks[lo], peaks[hi], q, times[near], kind, read_as)
+
+
+def design_table(names, line_areas, areas, peaks, times, kind: str = "unspecified") -> list[dict[str, object]]:
+    """One row per design line with a drainage area (wadi2d/arf.py:157-168). ``peaks``, ``times``: (runs x lines),
+    the runs in the order of ``areas``; a line whose area is None gets no row."""
+    peaks, times = np.asarray(peaks, np.float64), np.asarray(times, np.float64)
+    rows = []
+    for n, (name, area) in enumerate(zip(names, line_areas, strict=True)):
+        if area is None:
+            continue
+        rows.append(interpolated_row(name, float(area), areas, peaks[:, n], times[:, n], kind, READ_LINE))
+    return rows
+
+
+def log_area_weights(areas, area):
+    """The runs bracketing ``area`` (one value or one per cell) and the larger run's weight, linear in ln A
+    (wadi2d/arf.py:275-286): ``(low, high, w)``, read as ``(1 - w) * low + w * high``; beyond the runs the end run
+    holds (weight 0 or 1). ``areas`` rise and hold two at least."""
+    areas = np.asarray(areas, np.float64)
+    ln_runs = np.log(areas)
+    ln_at = np.log(np.clip(area, areas[0], areas[-1]))
+    high = np.clip(np.searchsorted(ln_runs, ln_at), 1, ln_runs.size - 1)
+    low = high - 1
+    return low, high, (ln_at - ln_runs[low]) / (ln_runs[high] - ln_runs[low])
+
+
+def composite_map(maps, areas, cell_area) -> np.ndarray:
+    """Per cell, the runs' maps read at the cell's drainage area (wadi2d/arf.py:289-297): the two runs that bracket it,
+    linear in ln A; beyond them the end run. One run: its map."""
+    areas = np.asarray(areas, np.float64)
+    if areas.size == 1:
+        return np.array(maps[0], dtype=np.float64)
+    low, high, w = log_area_weights(areas, cell_area)
+    stack = np.stack([np.asarray(m, np.float64) for m in maps])
+    j, i = np.indices(np.shape(cell_area), sparse=True)
+    return (1.0 - w) * stack[low, j, i] + w * stack[high, j, i]
+
+
+def composite_maps(envelopes: list[dict], areas, cell_area, depth_floor: float | None = None) -> dict[str, np.ndarray]:
+    """The study's composites (wadi2d/arf.py:300-316) from each run's envelope. With ``depth_floor``, a cell whose max
+    depth stays under it reads 0 in every map, as the reference reads a floored (no-data) cell of a run's map
+    (wadi2d/products/cell_maps.py:96-107, arf.py:311)."""
+    out = {}
+    for name in COMPOSITE_MAPS:
+        maps = []
+        for env in envelopes:
+            m = np.asarray(env[ENVELOPE_OF_MAP[name]], np.float64)
+            if depth_floor is not None:
+                m = np.where(np.asarray(env["depth"]) < depth_floor, 0.0, m)
+            maps.append(m)
+        out[name] = composite_map(maps, areas, cell_area)
+    return out
+
+
+# ------------------------------------------------------------------------------------------------ the runs
+
+
+@dataclass
+class StudyResult:
+    areas_km2: list[float]
+    peaks: np.ndarray  # (runs x lines) peak |Q|, m3/s
+    times: np.ndarray  # (runs x lines) time of the peak, s
+    table: list[dict[str, object]]
+    composite: dict[str, np.ndarray]
+    steps: np.ndarray
+    seconds: float
+    envelopes: list[dict] = field(default_factory=list)
+
+
+def storms_at(storm, areas) -> list:
+    """The study's storm at each storm area: the same storm with ``storm_area_km2`` set (its ARF table read there)."""
+    return [dataclasses.replace(storm, storm_area_km2=float(a)) for a in areas]
+
+
+def run_study(cat, storm, areas, line_names, line_areas, cell_area, t_end: float, window: float = 30.0,
+              every: int = 4, num=None, batched: bool = True, kind: str = "unspecified",
+              depth_floor: float | None = None) -> StudyResult:  # fmt: skip
+    """Every storm area of the study through the solver from dry ground to ``t_end``, then the design table and the
+    composites. ``cat``: the catchment (``critical.Catchment5``: grid, device tables, outfalls, outfall tally, rained
+    cells, design lines). ``batched``: all runs in one batch (the B200 form), else one plain run after another (the
+    reference's order). Seconds are CUDA-event time around the runs."""
+    import torch
+
+    from wadi2d_b200.config import Numerics
+
+    num = num or Numerics()
+    areas = [float(a) for a in areas]
+    storms = storms_at(storm, areas)
+    n, nl = len(areas), len(cat.lines)
+    peaks, times = np.zeros((n, nl)), np.zeros((n, nl))
+    steps = np.zeros(n, np.int64)
+    envelopes: list[dict] = []
+    lines = [ln[:4] for ln in cat.lines]
+    stream = torch.cuda.current_stream()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    if batched:
+        from wadi2d_b200.batch import Batch
+
+        B = Batch([cat.grid] * n, [cat.tables] * n, num)
+        B.set_boundary([cat.boundary] * n)
+        B.set_depth([np.zeros(cat.grid.shape)] * n)
+        B.set_tally([cat.tally] * n)
+        B.set_lines([lines] * n)
+        B.reset_envelope()
+        cells = [B.native_of(r, cat.rained) for r in range(n)]
+        torch.cuda.synchronize()
+        e0.record(stream)
+        B.run_windows(np.full(n, float(t_end)), storms, window=window, max_every=every, cells=cells)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        for r in range(n):
+            peaks[r], times[r] = B.line_peaks(r)
+            envelopes.append(B.envelope(r))
+        steps[:] = B.nsteps
+        del B
+    else:
+        from wadi2d_b200.maxima import Lines, Maxima, Tally
+        from wadi2d_b200.model import Model
+        from wadi2d_b200.run import DeviceRain, run_windows
+
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for r in range(n):
+            m = Model(cat.tables, num)
+            m.set_boundary(cat.boundary)
+            m.set_depth(np.zeros(cat.grid.shape))
+            tally = Tally(m, *cat.tally)
+            maxima = Maxima(m, 0.1, 0.05, every=every)
+            lines_r = Lines(m, lines)
+            rain = DeviceRain(m, storms[r], cat.rained)
+            run_windows(m, float(t_end), rain=rain, window=window, maxima=maxima, tally=tally)
+            peaks[r], times[r] = lines_r.peaks()
+            envelopes.append(maxima.fields())
+            steps[r] = m.stepper.nsteps
+            del m, tally, maxima, lines_r, rain
+        e1.record(stream)
+        torch.cuda.synchronize()
+    seconds = e0.elapsed_time(e1) / 1e3
+    table = design_table(line_names, line_areas, areas, peaks, times, kind)
+    composite = composite_maps(envelopes, areas, cell_area, depth_floor)
+    return StudyResult(areas, peaks, times, table, composite, steps, seconds, envelopes)
+
+
+def drainage_km2(cat) -> tuple[np.ndarray, np.ndarray]:
+    """Each cell's D8 drainage area, km2 (the study's accumulation raster), and each design line's (at its centre
+    cell)."""
+    from wadi2d_b200.critical import flow_accumulation
+
+    acc, _ = flow_accumulation(np.asarray(cat.tables.zmin), cat.grid.mask)
+    cell = acc * float(cat.grid.dx) ** 2 / 1e6
+    return cell, np.array([cell[j, i] for *_, (j, i) in cat.lines])
+
+
+def bracketing_areas(cat, ratio: float = 2.0, most: int = 8) -> tuple[list[float], np.ndarray, np.ndarray]:
+    """The study's storm areas bracketing the design lines' drainage areas (``arf.bracket``), with the cells' and the
+    lines' drainage areas."""
+    cell, line_a = drainage_km2(cat)
+    return bracket_areas(list(line_a), ratio, most), cell, line_a

@@ -649,9 +649,9 @@ def table_build(args) -> None:
 
 def arf_study(args) -> None:
     """The depth-area study (the reference's ``wadi2d arf``): configuration 5's catchment (a seeded fractal fan at
-    10 m with 4 x 4 pixels, 8 design lines on its channels), storm areas bracketing the lines' D8 drainage areas
-    (ratio 2, at most 8), a uniform 60 mm storm over 2 h read through an area-reduction table, 3 h from dry ground;
-    all storm areas as one batch against one run after another, CUDA-event time around the runs."""
+    10 m with 4 x 4 pixels, 8 design lines on its channels), six storm areas log-spaced from 0.1 to 30 km2, a uniform
+    60 mm storm over 2 h read through an area-reduction table at each, 3 h from dry ground; all storm areas as one
+    batch against one run after another, CUDA-event time around the runs."""
     import torch
 
     from wadi2d_b200 import critical as C
@@ -660,7 +660,8 @@ def arf_study(args) -> None:
 
     t0 = time.perf_counter()
     cat = C.prepare(n=args.study_n, dx=10.0, k=4, seed=17)
-    areas, cell, line_a = S.bracketing_areas(cat, ratio=2.0, most=8)
+    cell, line_a = S.drainage_km2(cat)
+    areas = S.storm_areas(list(line_a), n_areas=6, area_min_km2=0.1, area_max_km2=30.0)
     torch.cuda.synchronize()
     setup = time.perf_counter() - t0
     arf = ArfTable(np.array([0.1, 1.0, 10.0, 100.0, 1000.0]), np.array([1.0, 0.95, 0.86, 0.72, 0.55]))

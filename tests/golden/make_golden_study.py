@@ -7,8 +7,9 @@ Run in a container that holds the reference source tree (read-only is fine):
 
 The reference's study module (wadi2d/arf.py) imports its I/O stack (rasterio, h5py and the products) at the top, which
 this image does not have, so the script reads the module's source, takes the definitions of its pure numpy helpers
-(``bracket_areas``, ``run_name``, ``interpolate_peak``, ``_row``, ``interpolated_row``, ``log_area_weights``,
-``composite_map``) and executes those alone, with numpy. It writes ``study.npz`` (inputs and outputs) and
+(``bracket_areas``, ``storm_areas``, ``run_name``, ``interpolate_peak``, ``_row``, ``interpolated_row``,
+``log_area_weights``, ``composite_map``) and executes those alone, with numpy; ``storm_areas`` reads its job settings
+from stand-in records with the same attribute names. It writes ``study.npz`` (inputs and outputs) and
 ``study.json`` (the interpolated design rows and the run names). Nothing on the GPU side reads the reference.
 """
 
@@ -23,8 +24,8 @@ import numpy as np
 
 HERE = Path(__file__).resolve().parent
 REF = Path(os.environ.get("WADI2D_REFERENCE", "/root/reference"))
-WANTED = ("bracket_areas", "run_name", "interpolate_peak", "_row", "interpolated_row", "log_area_weights",
-          "composite_map")  # fmt: skip
+WANTED = ("bracket_areas", "storm_areas", "run_name", "interpolate_peak", "_row", "interpolated_row",
+          "log_area_weights", "composite_map")  # fmt: skip
 
 
 def reference_helpers() -> dict:
@@ -59,6 +60,29 @@ def main() -> None:
         for w, r, m in bracket_cases
     ]
     meta["run_names"] = {str(a): R["run_name"](a) for a in (0.5, 12.25, 1234.5678, 10.0)}
+
+    # storm_areas: the job's arf settings and design lines as stand-in records
+    from types import SimpleNamespace as NS
+
+    def cfg(lines, **arf):
+        base = dict(areas_km2=[], n_areas=6, area_min_km2=10.0, area_max_km2=600.0, bracket=False, by_arf_step=False,
+                    bracket_ratio=2.0, bracket_max=6, exact_points=False)  # fmt: skip
+        base.update(arf)
+        outs = NS(lines=[NS(drainage_area_km2=a) for a in lines])
+        return NS(arf=NS(**base), outputs=outs)
+
+    area_cases = [
+        ([3.3, None, 41.0], {}),
+        ([3.3, 41.0], {"areas_km2": [5.0, 2.0, 5.00001, 80.0]}),
+        ([3.3, 41.0], {"n_areas": 4, "area_min_km2": 0.1, "area_max_km2": 30.0}),
+        ([3.3, None, 41.0, 12.0], {"bracket": True, "bracket_ratio": 1.7, "bracket_max": 9}),
+        ([3.3, 41.0], {"bracket": True, "exact_points": True}),
+        ([0.25, 0.2], {"n_areas": 6, "area_min_km2": 0.1, "area_max_km2": 30.0, "exact_points": True}),
+    ]
+    meta["storm_areas"] = [
+        {"lines": lines, "arf": arf, "areas": [float(x) for x in R["storm_areas"](cfg(lines, **arf))]}
+        for lines, arf in area_cases
+    ]
 
     # interpolate_peak and interpolated_row
     areas = np.geomspace(1.0, 300.0, 7)

@@ -71,3 +71,11 @@ def test_composites_from_envelopes_with_a_depth_floor():
         a = np.where(envs[0]["depth"] < 0.5, 0.0, envs[0][field])
         b = np.where(envs[1]["depth"] < 0.5, 0.0, envs[1][field])
         assert np.allclose(out[name], (1 - w) * a + w * b, rtol=0, atol=1e-15)
+
+
+def test_storm_areas(gold):
+    _, meta = gold
+    for case in meta["storm_areas"]:
+        assert S.storm_areas(case["lines"], **case["arf"]) == case["areas"], case
+    with pytest.raises(ValueError):
+        S.storm_areas([None], bracket=True)

@@ -38,6 +38,26 @@ def bracket_areas(wanted, ratio: float, most: int) -> list[float]:
     return list(np.geomspace(lo, hi, min(max(gaps + 1, 2), most)))
 
 
+def storm_areas(lines_km2=(), areas_km2=(), n_areas: int = 6, area_min_km2: float = 10.0,
+                area_max_km2: float = 600.0, bracket: bool = False, bracket_ratio: float = 2.0, bracket_max: int = 6,
+                exact_points: bool = False) -> list[float]:  # fmt: skip
+    """A study's storm areas (wadi2d/arf.py:100-115, its ``arf`` settings as arguments, the defaults the reference's):
+    ``areas_km2`` as given, else ``n_areas`` log-spaced from ``area_min_km2`` to ``area_max_km2``; or, with
+    ``bracket``, areas bracketing the design lines' drainage areas ``lines_km2``; with ``exact_points`` the lines'
+    own areas too. Rounded to 1e-4 km2, sorted, each once. (The reference's ``by_arf_step`` placement, by equal steps
+    of the area-reduction factor, is not part of this.)"""
+    lines = [float(a) for a in lines_km2 if a is not None]
+    if bracket:
+        if not lines:
+            raise ValueError("arf.bracket needs a design line with a drainage area")
+        base = bracket_areas(lines, bracket_ratio, bracket_max)
+    else:
+        base = list(areas_km2) or list(np.geomspace(area_min_km2, area_max_km2, n_areas))
+    if exact_points:
+        base += lines
+    return sorted({round(float(x), 4) for x in base})
+
+
 def run_name(area: float) -> str:
     """A run folder's name for a storm area (wadi2d/arf.py:118-119): km2 with three decimals, the point as 'p'."""
     return ("A%010.3fkm2" % area).replace(".", "p")
@@ -236,8 +256,8 @@ def drainage_km2(cat) -> tuple[np.ndarray, np.ndarray]:
     return cell, np.array([cell[j, i] for *_, (j, i) in cat.lines])
 
 
-def bracketing_areas(cat, ratio: float = 2.0, most: int = 8) -> tuple[list[float], np.ndarray, np.ndarray]:
+def bracketing_areas(cat, ratio: float = 2.0, most: int = 6) -> tuple[list[float], np.ndarray, np.ndarray]:
     """The study's storm areas bracketing the design lines' drainage areas (``arf.bracket``), with the cells' and the
     lines' drainage areas."""
     cell, line_a = drainage_km2(cat)
-    return bracket_areas(list(line_a), ratio, most), cell, line_a
+    return storm_areas(list(line_a), bracket=True, bracket_ratio=ratio, bracket_max=most), cell, line_a

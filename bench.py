@@ -828,7 +828,9 @@ def main() -> None:
                        "l2": "inputs larger than L2 (about 15 GB resident)", "parallelism": f"replicas x{world}",
                        "loop": "device-resident, CUDA graphs of 16 steps"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
-            "gpu_launches": 8 * ran,
+            # the device loop's launches: the work list and the first step's settings, then graphs of 16 steps of
+            # six kernels (faces, update, envelope, boundary, control, plan)
+            "gpu_launches": 2 + 6 * 16 * -(-ran // 16),
         }  # fmt: skip
         print(json.dumps(line), flush=True)
     if world > 1:

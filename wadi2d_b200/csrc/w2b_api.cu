@@ -24,6 +24,7 @@ void launch_update(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s);
 __global__ void boundary_kernel(StepArgs A, int control);
 __global__ void envelope_kernel(StepArgs A);
 __global__ void clock_kernel(StepArgs A);
+__global__ void control_kernel(StepArgs A);
 __global__ void prestep_kernel(StepArgs A);
 __global__ void setstep_kernel(StepArgs A, float dtf, int want_wave, int want_wet, int nact);
 __global__ void endstep_kernel(StepArgs A);
@@ -257,13 +258,11 @@ static int launch_loop_step(Handle& H, cudaStream_t s) {
     A.list = A.work;
     const dim3 blk(32, 8);
     const int grid = blocks_for(H, H.g.ntiles - 1);
-    prestep_kernel<<<1, 1024, 0, s>>>(A);
     launch_faces(H.tmaps, A, faces_grid(H, H.g.ntiles - 1), s);
     launch_update(H.tmaps, A, grid, s);
     envelope_kernel<<<H.sms * 2, TILE2, 0, s>>>(A);
     boundary_kernel<<<boundary_grid(H, 1), 256, 0, s>>>(A, 1);
-    clock_kernel<<<1, 256, 0, s>>>(A);
-    activity_kernel<<<1, 1024, 0, s>>>(A, 0);
+    control_kernel<<<1, 1024, 0, s>>>(A);  // clocks, rebuild and work list, the next step's settings
     plan_kernel<<<grid, blk, 0, s>>>(A, A.woken, -1);
     CKL("loop step");
     return W2B_OK;
@@ -686,6 +685,7 @@ static int advance_runs(Handle* H, const W2BStepper* cfg, const double* t_end, i
     CK(cudaMemcpyAsync(R.refresh_due, rd.data(), 4 * n, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(R.status, st.data(), 4 * n, cudaMemcpyHostToDevice, s));
     activity_kernel<<<1, 1024, 0, s>>>(make_args(*H), 1);  // the work list of the runs that take a step
+    prestep_kernel<<<1, 1024, 0, s>>>(make_args(*H));      // the first step's settings; each step sets the next's
     CKL("advance work list");
     if (H->loop.version != H->version) {
         drop_graphs(*H);
@@ -722,7 +722,7 @@ static int advance_runs(Handle* H, const W2BStepper* cfg, const double* t_end, i
     std::vector<int32_t> par(n);
     CK(cudaMemcpyAsync(dt.data(), R.dt, 8 * n, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(ns.data(), R.nsteps, 8 * n, cudaMemcpyDeviceToHost, s));
-    CK(cudaMemcpyAsync(wb.data(), R.wave_bits, 4 * n, cudaMemcpyDeviceToHost, s));
+    CK(cudaMemcpyAsync(wb.data(), R.wave_last, 4 * n, cudaMemcpyDeviceToHost, s));
     CK(cudaMemcpyAsync(par.data(), R.parity, 4 * n, cudaMemcpyDeviceToHost, s));
     int32_t nact = 0;
     CK(cudaMemcpyAsync(&nact, &H->ctl()->nact, 4, cudaMemcpyDeviceToHost, s));

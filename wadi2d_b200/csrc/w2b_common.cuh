@@ -46,6 +46,7 @@ struct RunTab {
     int32_t *flags, *refresh_due, *status;
     uint32_t* wave_bits;  // max wave speed of the run's tiles, as float bits (waves are never negative)
     int32_t* parity;      // the run's current half of the ping-pong pairs
+    float* wave_last;     // the wave maximum of the run's last refresh step (what the clock reports)
 };
 
 // Whether run r takes another step (the loop test of wadi2d/solver/stepper.py:106, plus the batch's step limit).
@@ -56,7 +57,7 @@ __device__ __forceinline__ bool live_run(const RunTab& R, int r, const Ctl* ctl)
 // Layout of a run table of nruns entries in one device block: each array 256-byte aligned.
 __host__ __device__ inline size_t run_table_bytes(int nruns) {
     const size_t a = ((size_t)nruns * 8 + 255) / 256 * 256, b = ((size_t)nruns * 4 + 255) / 256 * 256;
-    return 8 * a + 8 * b;
+    return 8 * a + 9 * b;
 }
 
 __host__ __device__ inline RunTab run_table(void* base, int nruns) {
@@ -80,6 +81,7 @@ __host__ __device__ inline RunTab run_table(void* base, int nruns) {
     R.status = reinterpret_cast<int32_t*>(q + 5 * b);
     R.wave_bits = reinterpret_cast<uint32_t*>(q + 6 * b);
     R.parity = reinterpret_cast<int32_t*>(q + 7 * b);
+    R.wave_last = reinterpret_cast<float*>(q + 8 * b);
     return R;
 }
 

@@ -768,8 +768,8 @@ __global__ void boundary_kernel(StepArgs A, int control) {
 
 // Each running run's clock after its step (wadi2d/solver/stepper.py:113-124): the swap of its halves, t, the step
 // counts, the step rule on refresh steps (dt_min and non-finite checks); a run that stops marks the work list for
-// rebuilding. One CTA, after boundary_kernel.
-__global__ void clock_kernel(StepArgs A) {
+// rebuilding. The threads of one CTA, after boundary_kernel.
+__device__ void run_clocks(const StepArgs& A) {
     Ctl* ctl = A.ctl;
     if (!(ctl->any & ANY_RUN)) return;
     const RunTab& R = A.R;
@@ -780,6 +780,7 @@ __global__ void clock_kernel(StepArgs A) {
         R.nsteps[r] += 1;
         R.steps_run[r] += 1;
         if (R.flags[r] & F_WAVE) {
+            R.wave_last[r] = __uint_as_float(R.wave_bits[r]);
             const double w = (double)__uint_as_float(R.wave_bits[r]);
             if (!isfinite(w)) {
                 R.status[r] = W2B_ENONFINITE;
@@ -793,9 +794,11 @@ __global__ void clock_kernel(StepArgs A) {
     }
 }
 
+__global__ void clock_kernel(StepArgs A) { run_clocks(A); }
+
 // Before a step of the device loop, for each run: the loop test and the step's settings
-// (wadi2d/solver/stepper.py:106-111). One CTA; ctl->any gathers the runs' flags.
-__global__ void prestep_kernel(StepArgs A) {
+// (wadi2d/solver/stepper.py:106-111). The threads of one CTA; ctl->any gathers the runs' flags.
+__device__ void step_settings(const StepArgs& A) {
     Ctl* ctl = A.ctl;
     const RunTab& R = A.R;
     __shared__ uint32_t any;
@@ -829,6 +832,8 @@ __global__ void prestep_kernel(StepArgs A) {
     __syncthreads();
     if (threadIdx.x == 0) ctl->any = any;
 }
+
+__global__ void prestep_kernel(StepArgs A) { step_settings(A); }
 
 // The end of a host-driven step of run 0: the swap of the ping-pong pairs (wadi2d/solver/gpu/backend.py:185-188).
 __global__ void endstep_kernel(StepArgs A) { A.R.parity[0] ^= 1; }
@@ -876,10 +881,14 @@ __device__ __forceinline__ int block_scan(int flag, int* warp_sums, int* total) 
 // tiles that join the list are listed in woken for their wet share to be written. Then the work list: the active tiles
 // of the runs that take another step, rebuilt whenever the active list or the set of stepping runs changed.
 // only_work = 1: the work list alone, before the first step of the device loop.
-__global__ void __launch_bounds__(1024) activity_kernel(StepArgs A, int only_work) {
+__device__ void rebuild_lists(const StepArgs& A, int only_work) {
     Ctl* ctl = A.ctl;
     const bool rebuild = !only_work && (ctl->any & ANY_ACT);
-    if (!only_work && !rebuild && !ctl->prune) return;
+    if (!only_work && !rebuild) {
+        // no tile woke at this step: the plan pass that follows has nothing to do
+        if (threadIdx.x == 0) ctl->nwoken = 0;
+        if (!ctl->prune) return;
+    }
     const int nt = A.ntiles;
     int* wet_eff = A.scratch;
     int* flags = A.scratch + nt;
@@ -941,14 +950,24 @@ __global__ void __launch_bounds__(1024) activity_kernel(StepArgs A, int only_wor
     }
 }
 
+__global__ void __launch_bounds__(1024) activity_kernel(StepArgs A, int only_work) { rebuild_lists(A, only_work); }
+
+// The end of a step of the device loop and the settings of the next, in one CTA of 1024 threads: each running run's
+// clock, the active-list rebuild (for the runs that check at this step) with the woken tiles and the work list, then
+// the next step's loop test and settings. plan_kernel, after it, takes the woken tiles.
+__global__ void __launch_bounds__(1024) control_kernel(StepArgs A) {
+    run_clocks(A);
+    __syncthreads();
+    rebuild_lists(A, 0);
+    __syncthreads();
+    step_settings(A);
+}
+
 // refresh_plan of the listed tiles (wadi2d/solver/gpu/kernels/cells.cu:66-78) from the current mean depth. count < 0:
-// the tiles the device loop's rebuild woke (ctl->nwoken).
+// the tiles the device loop's last rebuild woke (ctl->nwoken, 0 when it did not rebuild).
 __global__ void __launch_bounds__(256) plan_kernel(StepArgs A, const int32_t* list, int count) {
     Ctl* ctl = A.ctl;
-    if (count < 0) {
-        if (!(ctl->any & ANY_ACT)) return;
-        count = ctl->nwoken;
-    }
+    if (count < 0) count = ctl->nwoken;
     for (int a = blockIdx.x; a < count; a += gridDim.x) {
         const int t = list[a];
         const int tj = A.tiles[2 * t], ti = A.tiles[2 * t + 1];

@@ -738,8 +738,13 @@ def main() -> None:
             dist.barrier()
         torch.cuda.synchronize(dev)
 
-    # warm-up: the graph capture and the first steps
+    # warm-up: the graph capture and the first steps; then the launch tuner settles (its candidate schedules give the
+    # same bits and differ only in time), so the timed steps run the schedule it kept
     m.run(1e12, maxima=maxima, tally=tally, max_steps=max(args.warmup, 3))
+    tune_steps = 0
+    while b.loop_config()["tuning"] and tune_steps < 4096:
+        m.run(1e12, maxima=maxima, tally=tally, max_steps=64)
+        tune_steps += 64
     barrier()
     phys = os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")
     clocks = Clocks(int(phys[local]) if len(phys) > local and phys[local].strip().isdigit() else local)
@@ -826,11 +831,12 @@ def main() -> None:
                                    "rain, every tile stepped, envelope every 4 steps, FP64 tally every step",
                        "cells": cells, "tiles": grid.ntiles - 1, "wet_fraction": wet, "cfl": m.num.cfl,
                        "l2": "inputs larger than L2 (about 15 GB resident)", "parallelism": f"replicas x{world}",
-                       "loop": "device-resident, CUDA graphs of 16 steps"},
+                       "loop": "device-resident, CUDA graphs", "launch": b.loop_config(),
+                       "tuning_steps": tune_steps},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
             # the device loop's launches: the work list and the first step's settings, then graphs of 16 steps of
             # six kernels (faces, update, envelope, boundary, control, plan)
-            "gpu_launches": 2 + 6 * 16 * -(-ran // 16),
+            "gpu_launches": 2 + 6 * b.loop_config()["steps_per_graph"] * -(-ran // b.loop_config()["steps_per_graph"]),
         }  # fmt: skip
         print(json.dumps(line), flush=True)
     if world > 1:

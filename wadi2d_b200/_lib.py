@@ -100,6 +100,8 @@ _SIGNATURES = {
     "w2b_set_run_dx": [c_vp, c_vp, c_i32],
     "w2b_run_halves": [c_vp, c_vp, c_vp],
     "w2b_face_waves": [c_vp, c_i32, c_f32, c_vp, c_vp],
+    "w2b_loop_tuning": [c_vp, c_i32, c_i32, c_i32, c_i32],
+    "w2b_loop_config": [c_vp, c_vp],
     "w2b_mma_gemm": [c_vp, c_vp, c_i32, c_i32, c_i32, c_vp, c_vp, c_vp, c_vp],
     "w2b_bf16_act": [c_vp, c_i64, c_i32, c_vp, c_vp],
     "w2b_relu_back": [c_vp, c_vp, c_i64, c_vp, c_vp],

@@ -39,9 +39,38 @@ __global__ void pack_tables_kernel(const float* dtab, const float* ftabx, const 
                                    float4* fx, float4* fy, int ntiles, int rows);
 __global__ void bmark_kernel(StepArgs A, int clear_words);
 
+// A launch configuration of the device loop: CTAs a SM of the face pass and of the update pass, and loop steps a
+// captured graph. Every configuration computes the same bits (a tile's arithmetic does not depend on the grid, and
+// the wave maximum is an order-free integer max); they differ only in time.
+struct LoopConfig {
+    int faces_per_sm, update_per_sm, steps;
+};
+constexpr int TUNE_CANDIDATES = 5;               // the default and one change of each knob either way
+constexpr int FORCED = TUNE_CANDIDATES;          // the slot of a configuration the caller fixes
+constexpr int TUNE_SAMPLES = 3;                  // timed graph launches a candidate before the tuner settles
+constexpr int MAX_GRAPH_STEPS = 64;
+constexpr double TUNE_MARGIN = 0.02;
+
+// The device loop's captured graphs, one a configuration, and the online tuner that picks among them: while tuning,
+// successive graph launches rotate through the candidates, each timed with CUDA events on the launching stream from
+// the end of the graph before it (so the host's read of the clocks between graphs counts against the configuration
+// whose graph follows it) and divided by the loop steps that ran (the empty steps of a graph that outlasts its runs
+// count against the configuration that spent them). Once every candidate has TUNE_SAMPLES launches, the fastest per
+// loop step is kept, the default unless another beats it by more than TUNE_MARGIN.
 struct Loop {
-    cudaGraphExec_t exec = nullptr;
-    unsigned version = ~0u;
+    LoopConfig cand[TUNE_CANDIDATES + 1];
+    int ncand = 0;
+    cudaGraphExec_t exec[TUNE_CANDIDATES + 1] = {};
+    unsigned version[TUNE_CANDIDATES + 1];
+    double sec[TUNE_CANDIDATES] = {};
+    long long steps[TUNE_CANDIDATES] = {};
+    int samples[TUNE_CANDIDATES] = {};
+    int next = 0, chosen = 0;
+    int tuning = 1;
+    cudaEvent_t ev[3] = {nullptr, nullptr, nullptr};  // a launch's start; the ends of two successive launches
+    Loop() {
+        for (auto& v : version) v = ~0u;
+    }
 };
 
 struct Handle {
@@ -67,6 +96,7 @@ struct Handle {
     int sms = 148;
     int step_blocks = 148;   // resident CTAs of the update pass
     int faces_blocks = 296;  // resident CTAs of the face pass
+    int faces_occ = 2, update_occ = 1;  // resident CTAs a SM of the two passes
     TMaps tmaps;
     unsigned version = 0;   // bumped whenever a graph would capture stale arguments
     Loop loop;
@@ -231,12 +261,37 @@ static int build_tmaps(Handle& H) {
     return st;
 }
 
-static void drop_graphs(Handle& H) {
-    if (H.loop.exec) {
-        cudaGraphExecDestroy(H.loop.exec);
-        H.loop.exec = nullptr;
+static void drop_graph(Handle& H, int c) {
+    if (H.loop.exec[c]) {
+        cudaGraphExecDestroy(H.loop.exec[c]);
+        H.loop.exec[c] = nullptr;
     }
-    H.loop.version = ~0u;
+    H.loop.version[c] = ~0u;
+}
+
+static void drop_graphs(Handle& H) {
+    for (int c = 0; c <= TUNE_CANDIDATES; ++c) drop_graph(H, c);
+}
+
+// The tuner's candidates: the occupancy-given default (both passes at their resident CTAs a SM, 16 steps a graph),
+// and from it one CTA a SM fewer in the face pass, half the update pass's, 8 and 32 steps a graph.
+static void init_loop(Handle& H) {
+    Loop& L = H.loop;
+    const int F = H.faces_occ, U = H.update_occ;
+    L.ncand = 0;
+    L.cand[L.ncand++] = {F, U, 16};
+    if (F > 1) L.cand[L.ncand++] = {F - 1, U, 16};
+    if (U > 1) L.cand[L.ncand++] = {F, (U + 1) / 2, 16};
+    L.cand[L.ncand++] = {F, U, 8};
+    L.cand[L.ncand++] = {F, U, 32};
+    L.cand[FORCED] = L.cand[0];
+    for (int c = 0; c < TUNE_CANDIDATES; ++c) {
+        L.sec[c] = 0.0;
+        L.steps[c] = 0;
+        L.samples[c] = 0;
+    }
+    L.next = L.chosen = 0;
+    L.tuning = 1;
 }
 
 // CTAs of boundary_kernel: enough for its items (boundary cells; with control, tally faces and a warp a line), at
@@ -252,14 +307,16 @@ static int boundary_grid(const Handle& H, int control) {
     return (int)(g < 1 ? 1 : (g > cap ? cap : g));
 }
 
-// One step of the device loop: every running run advances by one of its own steps.
-static int launch_loop_step(Handle& H, cudaStream_t s) {
+// One step of the device loop under launch configuration C: every running run advances by one of its own steps.
+static int launch_loop_step(Handle& H, const LoopConfig& C, cudaStream_t s) {
     StepArgs A = make_args(H);
     A.list = A.work;
     const dim3 blk(32, 8);
     const int grid = blocks_for(H, H.g.ntiles - 1);
-    launch_faces(H.tmaps, A, faces_grid(H, H.g.ntiles - 1), s);
-    launch_update(H.tmaps, A, grid, s);
+    const int tiles = H.g.ntiles - 1 > 0 ? H.g.ntiles - 1 : 1;
+    const int fgrid = H.sms * C.faces_per_sm, ugrid = H.sms * C.update_per_sm;
+    launch_faces(H.tmaps, A, tiles < fgrid ? tiles : fgrid, s);
+    launch_update(H.tmaps, A, tiles < ugrid ? tiles : ugrid, s);
     envelope_kernel<<<H.sms * 2, TILE2, 0, s>>>(A);
     boundary_kernel<<<boundary_grid(H, 1), 256, 0, s>>>(A, 1);
     control_kernel<<<1, 1024, 0, s>>>(A);  // clocks, rebuild and work list, the next step's settings
@@ -350,6 +407,9 @@ int32_t w2b_create(const W2BGridDesc* grid, const W2BParams* params, const W2BBu
     }
     const int focc = faces_occupancy();
     H->faces_blocks = H->sms * (focc > 0 ? focc : 1);
+    H->faces_occ = focc > 0 ? focc : 1;
+    H->update_occ = occ > 0 ? occ : 1;
+    init_loop(*H);
     if (build_tmaps(*H) != W2B_OK) {
         delete H;
         return W2B_ECUDA;
@@ -365,6 +425,14 @@ int32_t w2b_create(const W2BGridDesc* grid, const W2BParams* params, const W2BBu
         delete H;
         return cuda_status(cudaGetLastError(), "w2b_create stream");
     }
+    if (cudaEventCreate(&H->loop.ev[0]) != cudaSuccess || cudaEventCreate(&H->loop.ev[1]) != cudaSuccess ||
+        cudaEventCreate(&H->loop.ev[2]) != cudaSuccess) {
+        for (auto& e : H->loop.ev)
+            if (e) cudaEventDestroy(e);
+        cudaStreamDestroy(H->cap);
+        delete H;
+        return cuda_status(cudaGetLastError(), "w2b_create events");
+    }
     *handle = H;
     return cuda_status(cudaGetLastError(), "w2b_create");
 }
@@ -373,6 +441,8 @@ int32_t w2b_destroy(void* handle) {
     if (!handle) return W2B_EINVAL;
     Handle* H = static_cast<Handle*>(handle);
     drop_graphs(*H);
+    for (auto& e : H->loop.ev)
+        if (e) cudaEventDestroy(e);
     if (H->cap) cudaStreamDestroy(H->cap);
     delete H;
     return W2B_OK;
@@ -644,10 +714,50 @@ int32_t w2b_tally(void* handle, double dt, void* stream) {
     return W2B_OK;
 }
 
-// The device-resident loop. Steps run in chunks of a captured graph of LOOP_STEPS steps, every running run advancing
-// one of its own steps each graph step; after each chunk the host reads the runs' clocks once.
-static constexpr int LOOP_STEPS = 16;
+// The graph of configuration c, captured again when the arguments it would hold have changed.
+static int loop_graph(Handle& H, int c) {
+    Loop& L = H.loop;
+    if (L.exec[c] && L.version[c] == H.version) return W2B_OK;
+    drop_graph(H, c);
+    cudaGraph_t graph;
+    CK(cudaStreamBeginCapture(H.cap, cudaStreamCaptureModeThreadLocal));
+    int stc = W2B_OK;
+    for (int k = 0; k < L.cand[c].steps && stc == W2B_OK; ++k) stc = launch_loop_step(H, L.cand[c], H.cap);
+    cudaError_t e = cudaStreamEndCapture(H.cap, &graph);
+    if (stc != W2B_OK) return stc;
+    CK(e);
+    e = cudaGraphInstantiate(&L.exec[c], graph, 0);
+    cudaGraphDestroy(graph);
+    CK(e);
+    L.version[c] = H.version;
+    return W2B_OK;
+}
 
+// One timed launch of candidate c ran `live` loop steps in `ms`: add it, move to the next candidate, and settle on the
+// fastest once every candidate has its samples.
+static void tune_sample(Handle& H, int c, long long live, float ms) {
+    Loop& L = H.loop;
+    if (live > 0) {
+        L.sec[c] += 1e-3 * (double)ms;
+        L.steps[c] += live;
+        L.samples[c] += 1;
+    }
+    L.next = (c + 1) % L.ncand;
+    for (int k = 0; k < L.ncand; ++k)
+        if (L.samples[k] < TUNE_SAMPLES) return;
+    auto per_step = [&](int k) { return L.sec[k] / (double)(L.steps[k] > 0 ? L.steps[k] : 1); };
+    int best = 0;
+    for (int k = 1; k < L.ncand; ++k)
+        if (per_step(k) < per_step(best)) best = k;
+    if (best != 0 && !(per_step(best) < (1.0 - TUNE_MARGIN) * per_step(0))) best = 0;
+    L.chosen = best;
+    L.tuning = 0;
+    for (int k = 0; k < L.ncand; ++k)
+        if (k != best) drop_graph(H, k);
+}
+
+// The device-resident loop. Steps run in chunks of a captured graph (the launch configuration's steps), every running
+// run advancing one of its own steps each graph step; after each chunk the host reads the runs' clocks once.
 static int advance_runs(Handle* H, const W2BStepper* cfg, const double* t_end, int64_t max_steps, W2BClock* clocks,
                         cudaStream_t s) {
     const int n = H->nruns;
@@ -687,29 +797,41 @@ static int advance_runs(Handle* H, const W2BStepper* cfg, const double* t_end, i
     activity_kernel<<<1, 1024, 0, s>>>(make_args(*H), 1);  // the work list of the runs that take a step
     prestep_kernel<<<1, 1024, 0, s>>>(make_args(*H));      // the first step's settings; each step sets the next's
     CKL("advance work list");
-    if (H->loop.version != H->version) {
-        drop_graphs(*H);
-        cudaGraph_t graph;
-        CK(cudaStreamBeginCapture(H->cap, cudaStreamCaptureModeThreadLocal));
-        int stc = W2B_OK;
-        for (int k = 0; k < LOOP_STEPS && stc == W2B_OK; ++k) stc = launch_loop_step(*H, H->cap);
-        cudaError_t e = cudaStreamEndCapture(H->cap, &graph);
-        if (stc != W2B_OK) return stc;
-        CK(e);
-        e = cudaGraphInstantiate(&H->loop.exec, graph, 0);
-        cudaGraphDestroy(graph);
-        CK(e);
-        H->loop.version = H->version;
-    }
+    Loop& L = H->loop;
     std::vector<long long> run(n);
+    long long ran_before = 0;  // loop steps so far in this call (the largest steps_run of any run)
     int32_t gstatus = 0;
+    int end = 1, have_prev = 0;  // ev[end] takes this launch's end; ev[3 - end] holds the last one's, if have_prev
+    if (L.tuning)  // every candidate's graph before the first timed launch: no capture falls inside a timing
+        for (int k = 0; k < L.ncand; ++k) {
+            const int stc = loop_graph(*H, k);
+            if (stc != W2B_OK) return stc;
+        }
     for (;;) {
-        CK(cudaGraphLaunch(H->loop.exec, s));
+        const bool timed = L.tuning != 0;
+        const int c = timed ? L.next : L.chosen;
+        const int stc = loop_graph(*H, c);
+        if (stc != W2B_OK) return stc;
+        if (timed && !have_prev) CK(cudaEventRecord(L.ev[0], s));
+        CK(cudaGraphLaunch(L.exec[c], s));
+        if (timed) CK(cudaEventRecord(L.ev[end], s));
         CK(cudaMemcpyAsync(t.data(), R.t, 8 * n, cudaMemcpyDeviceToHost, s));
         CK(cudaMemcpyAsync(run.data(), R.steps_run, 8 * n, cudaMemcpyDeviceToHost, s));
         CK(cudaMemcpyAsync(st.data(), R.status, 4 * n, cudaMemcpyDeviceToHost, s));
         CK(cudaMemcpyAsync(&gstatus, &H->ctl()->status, 4, cudaMemcpyDeviceToHost, s));
         CK(cudaStreamSynchronize(s));
+        if (timed) {
+            long long ran = 0;
+            for (int r = 0; r < n; ++r) ran = run[r] > ran ? run[r] : ran;
+            float ms = 0.0f;
+            CK(cudaEventElapsedTime(&ms, have_prev ? L.ev[3 - end] : L.ev[0], L.ev[end]));
+            tune_sample(*H, c, ran - ran_before, ms);
+            ran_before = ran;
+            have_prev = 1;
+            end = 3 - end;
+        } else {
+            have_prev = 0;
+        }
         bool done = gstatus != 0;
         if (!done) {
             done = true;
@@ -758,6 +880,39 @@ int32_t w2b_advance_runs(void* handle, const W2BStepper* cfg, const double* t_en
     if (!handle || !cfg || !clocks || !t_end || max_steps < 0 || cfg->dt_every < 1 || cfg->active_every < 1)
         return W2B_EINVAL;
     return advance_runs(static_cast<Handle*>(handle), cfg, t_end, max_steps, clocks, (cudaStream_t)stream);
+}
+
+int32_t w2b_loop_tuning(void* handle, int32_t tune, int32_t faces_per_sm, int32_t update_per_sm, int32_t steps) {
+    if (!handle) return W2B_EINVAL;
+    Handle* H = static_cast<Handle*>(handle);
+    Loop& L = H->loop;
+    if (tune) {
+        drop_graphs(*H);
+        init_loop(*H);
+        return W2B_OK;
+    }
+    if (faces_per_sm < 1 || faces_per_sm > H->faces_occ || update_per_sm < 1 || update_per_sm > H->update_occ ||
+        steps < 1 || steps > MAX_GRAPH_STEPS)
+        return W2B_EINVAL;
+    L.cand[FORCED] = {faces_per_sm, update_per_sm, steps};
+    drop_graph(*H, FORCED);
+    L.chosen = FORCED;
+    L.tuning = 0;
+    return W2B_OK;
+}
+
+int32_t w2b_loop_config(void* handle, int32_t* out) {
+    if (!handle || !out) return W2B_EINVAL;
+    const Handle* H = static_cast<const Handle*>(handle);
+    const Loop& L = H->loop;
+    const LoopConfig& C = L.cand[L.tuning ? L.next : L.chosen];
+    out[0] = C.faces_per_sm;
+    out[1] = C.update_per_sm;
+    out[2] = C.steps;
+    out[3] = L.tuning;
+    out[4] = H->faces_occ;
+    out[5] = H->update_occ;
+    return W2B_OK;
 }
 
 int32_t w2b_face_waves(void* handle, int32_t tile, float dt, float* out, void* stream) {

@@ -54,7 +54,7 @@ def parse():
     p.add_argument("--n", type=int, default=4096, help="domain side in cells (configuration 3: 4096)")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--e2e-windows", type=int, default=4)
+    p.add_argument("--e2e-windows", type=int, default=16)
     p.add_argument("--full-run", action="store_true",
                    help="the whole 36 h run of configuration 3 from dry ground, with its mass balance")
     p.add_argument("--sim-hours", type=float, default=36.0, help="--full-run: simulated hours (configuration 3: 36)")

@@ -2,8 +2,6 @@
 
 from __future__ import annotations
 
-import numpy as np
-
 from oracle import oracle as O
 
 

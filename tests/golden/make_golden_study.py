@@ -18,6 +18,7 @@ from __future__ import annotations
 import ast
 import json
 import os
+import sys
 from pathlib import Path
 
 import numpy as np
@@ -61,12 +62,31 @@ def main() -> None:
     ]
     meta["run_names"] = {str(a): R["run_name"](a) for a in (0.5, 12.25, 1234.5678, 10.0)}
 
+    # ArfTable.step_areas (wadi2d/storm/arf.py imports numpy only, so it is imported as it stands)
+    sys.path.insert(0, str(REF))
+    from wadi2d.storm.arf import ArfTable
+
+    step_tables = [
+        ([1.0, 10.0, 100.0, 1000.0], [1.0, 0.9, 0.75, 0.6], True),
+        ([5.0, 20.0, 80.0], [0.95, 0.7, 0.8], True),  # a factor that rises again
+        ([5.0, 20.0, 80.0], [0.9, 0.8, 0.6], False),  # the full depth below the table
+    ]
+    step_cases = [(0, 2.0, 500.0, 0.05), (0, 30.0, 40.0, 0.05), (0, 7.0, 7.0, 0.05), (1, 1.0, 200.0, 0.03),
+                  (2, 1.0, 200.0, 0.04), (2, 10.0, 60.0, 0.5), (0, 0.5, 3000.0, 0.02)]  # fmt: skip
+    meta["step_tables"] = step_tables
+    meta["step_areas"] = [
+        {"table": t, "low": lo, "high": hi, "step": st,
+         "areas": ArfTable(np.array(step_tables[t][0]), np.array(step_tables[t][1]), step_tables[t][2]).step_areas(
+             lo, hi, st)}
+        for t, lo, hi, st in step_cases
+    ]  # fmt: skip
+
     # storm_areas: the job's arf settings and design lines as stand-in records
     from types import SimpleNamespace as NS
 
     def cfg(lines, **arf):
         base = dict(areas_km2=[], n_areas=6, area_min_km2=10.0, area_max_km2=600.0, bracket=False, by_arf_step=False,
-                    bracket_ratio=2.0, bracket_max=6, exact_points=False)  # fmt: skip
+                    bracket_ratio=2.0, bracket_max=6, exact_points=False, arf_step_max=0.05)  # fmt: skip
         base.update(arf)
         outs = NS(lines=[NS(drainage_area_km2=a) for a in lines])
         return NS(arf=NS(**base), outputs=outs)
@@ -82,6 +102,18 @@ def main() -> None:
     meta["storm_areas"] = [
         {"lines": lines, "arf": arf, "areas": [float(x) for x in R["storm_areas"](cfg(lines, **arf))]}
         for lines, arf in area_cases
+    ]
+    # by_arf_step: the module's arf_step_areas reads the job's storm table; here it reads the first step table
+    step_table = ArfTable(np.array(step_tables[0][0]), np.array(step_tables[0][1]), step_tables[0][2])
+    R["arf_step_areas"] = lambda job, low, high: step_table.step_areas(low, high, job.arf.arf_step_max)
+    arf_step_cases = [
+        ([3.3, None, 41.0], {"by_arf_step": True}),
+        ([3.3, 410.0, 12.0], {"by_arf_step": True, "arf_step_max": 0.02, "exact_points": True}),
+        ([3.3, 41.0], {"by_arf_step": True, "bracket": True}),  # the bracket rule comes first
+    ]
+    meta["storm_areas_by_step"] = [
+        {"lines": lines, "arf": arf, "areas": [float(x) for x in R["storm_areas"](cfg(lines, **arf))]}
+        for lines, arf in arf_step_cases
     ]
 
     # interpolate_peak and interpolated_row

@@ -79,3 +79,18 @@ def test_storm_areas(gold):
         assert S.storm_areas(case["lines"], **case["arf"]) == case["areas"], case
     with pytest.raises(ValueError):
         S.storm_areas([None], bracket=True)
+
+
+def test_arf_step_areas_and_the_by_step_placement(gold):
+    from wadi2d_b200.forcing import ArfTable
+
+    _, meta = gold
+    tables = [ArfTable(np.array(a), np.array(f), r) for a, f, r in meta["step_tables"]]
+    for case in meta["step_areas"]:
+        assert tables[case["table"]].step_areas(case["low"], case["high"], case["step"]) == case["areas"], case
+    with pytest.raises(ValueError):
+        tables[0].step_areas(1.0, 2.0, 0.0)
+    for case in meta["storm_areas_by_step"]:
+        assert S.storm_areas(case["lines"], table=tables[0], **case["arf"]) == case["areas"], case
+    with pytest.raises(ValueError):
+        S.storm_areas([3.0, 9.0], by_arf_step=True)  # no table to place the areas by

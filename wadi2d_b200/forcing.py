@@ -86,6 +86,34 @@ class ArfTable:
             return 1.0
         return float(np.interp(area_km2, self.areas_km2, self.factors))
 
+    def step_areas(self, low_km2: float, high_km2: float, largest_change: float) -> list[float]:
+        """Storm areas from ``low_km2`` to ``high_km2``, both in, with the factor (as ``factor`` reads it) changing by
+        at most ``largest_change`` between neighbours, in as few areas as that allows (wadi2d/storm/arf.py:39-67). The
+        factor's whole path over the span, its rises and falls both counted, is cut into equal steps, and each cut is
+        placed by linear interpolation along the path between the table's areas."""
+        if not largest_change > 0.0:
+            raise ValueError("the largest change of the area-reduction factor must be above zero")
+        lo, hi = float(low_km2), float(high_km2)
+        if hi <= lo * (1.0 + 1e-9):
+            return [lo]
+        knots = sorted({lo, hi, *(float(a) for a in self.areas_km2 if lo < a < hi)})
+        vals = [self.factor(a) for a in knots]
+        first = float(self.areas_km2[0])
+        if not self.reduces_below_table and lo < first < hi:  # the full depth holds up to just below the table
+            at = knots.index(first)
+            knots.insert(at, first)
+            vals.insert(at, 1.0)
+        path = np.concatenate(([0.0], np.cumsum(np.abs(np.diff(vals)))))
+        n = max(1, int(np.ceil(path[-1] / largest_change - 1e-9)))
+        out = [lo]
+        for target in path[-1] * np.arange(1, n) / n:
+            k = min(max(int(np.searchsorted(path, target, side="left")), 1), len(knots) - 1)
+            seg = path[k] - path[k - 1]
+            share = (target - path[k - 1]) / seg if seg > 0 else 1.0
+            out.append(float(knots[k - 1] + share * (knots[k] - knots[k - 1])))
+        out.append(hi)
+        return sorted(set(out))
+
 
 @dataclass(frozen=True)
 class GivenFactor:

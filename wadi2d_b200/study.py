@@ -40,17 +40,25 @@ def bracket_areas(wanted, ratio: float, most: int) -> list[float]:
 
 def storm_areas(lines_km2=(), areas_km2=(), n_areas: int = 6, area_min_km2: float = 10.0,
                 area_max_km2: float = 600.0, bracket: bool = False, bracket_ratio: float = 2.0, bracket_max: int = 6,
-                exact_points: bool = False) -> list[float]:  # fmt: skip
-    """A study's storm areas (wadi2d/arf.py:100-115, its ``arf`` settings as arguments, the defaults the reference's):
+                exact_points: bool = False, by_arf_step: bool = False, arf_step_max: float = 0.05,
+                table=None) -> list[float]:  # fmt: skip
+    """A study's storm areas (wadi2d/arf.py:89-115, its ``arf`` settings as arguments, the defaults the reference's):
     ``areas_km2`` as given, else ``n_areas`` log-spaced from ``area_min_km2`` to ``area_max_km2``; or, with
-    ``bracket``, areas bracketing the design lines' drainage areas ``lines_km2``; with ``exact_points`` the lines'
-    own areas too. Rounded to 1e-4 km2, sorted, each once. (The reference's ``by_arf_step`` placement, by equal steps
-    of the area-reduction factor, is not part of this.)"""
+    ``bracket``, areas bracketing the design lines' drainage areas ``lines_km2``; or, with ``by_arf_step``, areas
+    over the lines' span placed so that the storm's area-reduction ``table`` (a ``forcing.ArfTable``) changes by at
+    most ``arf_step_max`` between neighbours; with ``exact_points`` the lines' own areas too. Rounded to 1e-4 km2,
+    sorted, each once."""
     lines = [float(a) for a in lines_km2 if a is not None]
-    if bracket:
+    if bracket or by_arf_step:
         if not lines:
-            raise ValueError("arf.bracket needs a design line with a drainage area")
-        base = bracket_areas(lines, bracket_ratio, bracket_max)
+            rule = "arf.bracket" if bracket else "arf.by_arf_step"
+            raise ValueError(f"{rule} needs a design line with a drainage area")
+        if bracket:
+            base = bracket_areas(lines, bracket_ratio, bracket_max)
+        else:
+            if table is None or not hasattr(table, "step_areas"):
+                raise ValueError("arf.by_arf_step needs the storm's area-reduction table: the areas are placed by it")
+            base = table.step_areas(min(lines), max(lines), arf_step_max)
     else:
         base = list(areas_km2) or list(np.geomspace(area_min_km2, area_max_km2, n_areas))
     if exact_points:

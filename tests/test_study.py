@@ -94,3 +94,17 @@ def test_arf_step_areas_and_the_by_step_placement(gold):
         assert S.storm_areas(case["lines"], table=tables[0], **case["arf"]) == case["areas"], case
     with pytest.raises(ValueError):
         S.storm_areas([3.0, 9.0], by_arf_step=True)  # no table to place the areas by
+
+
+def test_a_study_refuses_storms_that_make_identical_runs():
+    from wadi2d_b200.forcing import ArfTable, GivenFactor, UniformStorm
+
+    table = ArfTable(np.array([1.0, 10.0, 100.0]), np.array([1.0, 0.9, 0.7]))
+    S.check_study(UniformStorm(50.0, 60.0, arf=table), [2.0, 20.0])
+    for storm in (UniformStorm(50.0, 60.0), UniformStorm(50.0, 60.0, arf=GivenFactor(0.8))):
+        with pytest.raises(ValueError):
+            S.check_study(storm, [2.0, 20.0])
+    flat = ArfTable(np.array([1.0, 10.0]), np.array([0.8, 0.8]))
+    with pytest.raises(ValueError):
+        S.check_study(UniformStorm(50.0, 60.0, arf=flat), [2.0, 5.0])
+    S.check_study(UniformStorm(50.0, 60.0, arf=flat), [2.0])  # one area: one run

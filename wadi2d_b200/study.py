@@ -180,6 +180,24 @@ class StudyResult:
     envelopes: list[dict] = field(default_factory=list)
 
 
+def check_study(storm, areas) -> None:
+    """A study needs a storm with an area-reduction table that tells its runs apart (wadi2d/arf.py:319-349,
+    :374-383): a single given factor, no table, or the same depth at every storm area would make every run the same
+    run. Raises ValueError."""
+    from wadi2d_b200.forcing import ArfTable, GivenFactor
+
+    arf = getattr(storm, "arf", None)
+    if isinstance(arf, GivenFactor):
+        raise ValueError("a depth-area study reads the area-reduction table at each storm area; a given factor is one "
+                         "factor at every area, so every run would be the same run")  # fmt: skip
+    if not isinstance(arf, ArfTable):
+        raise ValueError("a depth-area study needs the storm's area-reduction table: without it every run is the same")
+    depths = {round(s.total_depth, 9) for s in storms_at(storm, areas)}
+    if len(areas) > 1 and len(depths) == 1:
+        raise ValueError(f"the area-reduction table gives one factor at all the storm areas {list(areas)}: the runs "
+                         "would be identical")  # fmt: skip
+
+
 def storms_at(storm, areas) -> list:
     """The study's storm at each storm area: the same storm with ``storm_area_km2`` set (its ARF table read there)."""
     return [dataclasses.replace(storm, storm_area_km2=float(a)) for a in areas]
@@ -198,6 +216,7 @@ def run_study(cat, storm, areas, line_names, line_areas, cell_area, t_end: float
 
     num = num or Numerics()
     areas = [float(a) for a in areas]
+    check_study(storm, areas)
     storms = storms_at(storm, areas)
     n, nl = len(areas), len(cat.lines)
     peaks, times = np.zeros((n, nl)), np.zeros((n, nl))

@@ -108,3 +108,23 @@ def test_a_study_refuses_storms_that_make_identical_runs():
     with pytest.raises(ValueError):
         S.check_study(UniformStorm(50.0, 60.0, arf=flat), [2.0, 5.0])
     S.check_study(UniformStorm(50.0, 60.0, arf=flat), [2.0])  # one area: one run
+
+
+def test_study_outputs_in_the_reference_layout(tmp_path, gold):
+    import csv
+
+    g, meta = gold
+    rows = [meta["rows"][2], meta["rows"][4]]
+    res = S.StudyResult([1.0, 3.0], np.zeros((2, 2)), np.zeros((2, 2)), rows,
+                        {"max_depth": np.ones((3, 4)), "max_speed": np.zeros((3, 4)), "hazard": np.zeros((3, 4))},
+                        np.array([5, 6]), 0.0)  # fmt: skip
+    paths = S.write_study(tmp_path / "study1", res, "storm-centred")
+    with open(paths["table"], newline="", encoding="utf-8") as f:
+        back = list(csv.DictReader(f))
+    assert list(back[0]) == list(rows[0])
+    assert [float(r["design_peak_m3s"]) for r in back] == [r["design_peak_m3s"] for r in rows]
+    study = __import__("json").loads(paths["study"].read_text())
+    assert study["areas_km2"] == [1.0, 3.0] and study["arf_table_type"] == "storm-centred" and study["table"] == rows
+    assert np.array_equal(np.load(paths["max_depth"]), np.ones((3, 4)))
+    S.write_table(tmp_path / "empty.csv", [])
+    assert (tmp_path / "empty.csv").read_text() == "design_point\n"

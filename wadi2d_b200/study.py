@@ -7,8 +7,9 @@ maps against an accumulation raster (``composite_maps``, arf.py:300-316). Here t
 of device tables and go into one ``Batch``: each run is the same storm with its storm area set to one of the study's
 areas (the ARF table read there), its own clock, envelope and design lines, and each run steps exactly as it would
 alone. The readings below keep the reference's names, arguments and results (pinned by ``tests/test_study.py``
-against the reference's own functions); the job file, GeoTIFF and progress-file plumbing around them is the
-reference's run driver and stays there.
+against the reference's own functions), and ``write_study`` writes ``design_points.csv`` and ``study.json`` as the
+reference does; the job file, the GeoTIFF maps and the progress file around them are the reference's run driver and
+stay there.
 """
 
 from __future__ import annotations
@@ -281,6 +282,44 @@ def drainage_km2(cat) -> tuple[np.ndarray, np.ndarray]:
     acc, _ = flow_accumulation(np.asarray(cat.tables.zmin), cat.grid.mask)
     cell = acc * float(cat.grid.dx) ** 2 / 1e6
     return cell, np.array([cell[j, i] for *_, (j, i) in cat.lines])
+
+
+def write_table(path, rows: list[dict[str, object]]) -> None:
+    """``design_points.csv`` (wadi2d/arf.py:186-195): a header of the rows' keys and a line a row; with no rows, the
+    header ``design_point`` alone."""
+    import csv
+    from pathlib import Path
+
+    path = Path(path)
+    path.parent.mkdir(parents=True, exist_ok=True)
+    with path.open("w", newline="", encoding="utf-8") as f:
+        if not rows:
+            f.write("design_point\n")
+            return
+        writer = csv.DictWriter(f, fieldnames=list(rows[0]))
+        writer.writeheader()
+        writer.writerows(rows)
+
+
+def write_study(folder, res: StudyResult, kind: str = "unspecified") -> dict:
+    """A study's outputs into ``folder`` as the reference lays them out (wadi2d/arf.py:383-395): ``design_points.csv``,
+    ``study.json`` (storm areas, the table's type, the rows, no on-grid elements) and one composite per quantity under
+    ``composite/``, as ``.npy`` arrays on the cell grid (the reference writes GeoTIFF through rasterio, which this
+    package does not carry). Returns the paths."""
+    import json
+    from pathlib import Path
+
+    folder = Path(folder)
+    folder.mkdir(parents=True, exist_ok=True)
+    write_table(folder / "design_points.csv", res.table)
+    study = {"areas_km2": res.areas_km2, "arf_table_type": kind, "table": res.table, "on_grid": []}
+    (folder / "study.json").write_text(json.dumps(study, indent=2), encoding="utf-8")
+    out = {"table": folder / "design_points.csv", "study": folder / "study.json"}
+    (folder / "composite").mkdir(exist_ok=True)
+    for name, data in res.composite.items():
+        out[name] = folder / "composite" / f"{name}.npy"
+        np.save(out[name], np.asarray(data, np.float64))
+    return out
 
 
 def bracketing_areas(cat, ratio: float = 2.0, most: int = 6) -> tuple[list[float], np.ndarray, np.ndarray]:

@@ -4,9 +4,9 @@
 records them, the envelope and the outfall volume) at chosen step counts: configuration 1 (``c1_small``: rain on a
 V-channel plane, free outfall, CFL 0.9, sleeping tiles, the envelope every 4 steps) or the crest case (``crest``:
 crest caps, walls, fixed-stage and follow boundaries). ``compare`` measures a float32 run's snapshot against the FP64
-run's (oracle/fp64.py, replaying the float32 run's own dt sequence) with the north star's bounds: the wet set and the
-crest-blocked faces identical, depth within 1e-4 relative or 1e-5 m, and unit discharge within 1e-4 of its field's
-scale.
+run's (oracle/fp64.py, replaying the float32 run's own dt sequence) with the step's accuracy bounds: the wet set and
+the crest-blocked faces identical, depth within 1e-4 relative or 1e-5 m, and unit discharge within 1e-4 of its
+field's scale.
 """
 
 from __future__ import annotations
@@ -88,7 +88,7 @@ def crest_faces() -> tuple[np.ndarray, np.ndarray]:
 
 
 def compare(s32: dict, s64: dict, crest: tuple | None = None) -> dict:
-    """The float32 snapshot against the FP64 one: per-field errors and the north star's checks (with ``crest``, the
+    """The float32 snapshot against the FP64 one: per-field errors and the accuracy checks (with ``crest``, the
     crest faces' masks, also the set of crest faces that carry no discharge)."""
     out = {"fields": {}}
     for key in s32:

@@ -13,7 +13,7 @@ from oracle_api import OracleApi
 MARKS = (100, 200)
 
 
-def test_float32_oracle_within_the_north_star_bounds_of_the_fp64_run():
+def test_float32_oracle_within_the_accuracy_bounds_of_the_fp64_run():
     s32, dts = F.snapshots(OracleApi(), MARKS, n=64)
     s64 = F.fp64_snapshots(dts, MARKS, n=64)
     for k in MARKS:

@@ -1,7 +1,7 @@
 """Configuration 2 at a reduced size on the B200: crest faces from seeded breaklines, three lumped inflows shared over
 their cells by depth through the window driver (wadi2d/forcing.py:667-695, depths read from the device as
 wadi2d/forcing.py:631-644 does), a reservoir started at its level (hbar_at_level), Manning patches and a free outfall.
-The step on the oracle's tables against the oracle's run field by field within the north star's tolerances, the
+The step on the oracle's tables against the oracle's run field by field within the step's accuracy tolerances, the
 GPU-built tables against the oracle's within one ulp, and the FP64 books closing."""
 
 from __future__ import annotations

@@ -1,4 +1,4 @@
-"""The CUDA path against the FP64 run (oracle/fp64.py), with the north star's bounds: configuration 1 at its full
+"""The CUDA path against the FP64 run (oracle/fp64.py), with the step's accuracy bounds: configuration 1 at its full
 size (256 x 256 cells, 5 x 5 pixels) after 200 steps, and the crest case after 100 steps. The FP64 run replays the
 CUDA run's own dt sequence, so the two differ only by arithmetic precision."""
 
@@ -12,7 +12,7 @@ from product_api import B200Api
 pytestmark = pytest.mark.gpu
 
 
-def test_configuration1_within_the_north_star_bounds_of_the_fp64_run():
+def test_configuration1_within_the_accuracy_bounds_of_the_fp64_run():
     s32, dts = F.snapshots(B200Api(), (200,), n=256)
     s64 = F.fp64_snapshots(dts, (200,), n=256)
     r = F.compare(s32[200], s64[200])

@@ -1,7 +1,7 @@
 """The CUDA path against the reference's own outputs (the golden cases) and against the oracle.
 
-Tolerances are the north star's: the wet set and the active tiles identical; depth within 1e-5 m absolute; unit
-discharge and velocity within 1e-4 relative of the field's scale. The arithmetic is the reference CPU twin's statement
+Tolerances: the wet set and the active tiles identical; depth within 1e-5 m absolute; unit discharge and velocity
+within 1e-4 relative of the field's scale. The arithmetic is the reference CPU twin's statement
 for statement, so the step count and every dt are expected to match exactly, and they are asserted so.
 """
 

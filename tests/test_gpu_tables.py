@@ -1,5 +1,5 @@
 """The GPU table builder against the reference's tables (pinned through the oracle, bit for bit to the reference):
-every array within one float32 ulp, and the step on GPU-built tables within the north star's tolerances of the
+every array within one float32 ulp, and the step on GPU-built tables within the step's accuracy tolerances of the
 reference's run. CUDA's double cbrt and pow may round the last bit of a double differently from glibc's; a float32
 table entry then differs by at most one ulp, and only rarely."""
 

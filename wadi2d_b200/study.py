@@ -204,22 +204,17 @@ def storms_at(storm, areas) -> list:
     return [dataclasses.replace(storm, storm_area_km2=float(a)) for a in areas]
 
 
-def run_study(cat, storm, areas, line_names, line_areas, cell_area, t_end: float, window: float = 30.0,
-              every: int = 4, num=None, batched: bool = True, kind: str = "unspecified",
-              depth_floor: float | None = None) -> StudyResult:  # fmt: skip
-    """Every storm area of the study through the solver from dry ground to ``t_end``, then the design table and the
-    composites. ``cat``: the catchment (``critical.Catchment5``: grid, device tables, outfalls, outfall tally, rained
-    cells, design lines). ``batched``: all runs in one batch (the B200 form), else one plain run after another (the
-    reference's order). Seconds are CUDA-event time around the runs."""
+def solve_runs(cat, storms: list, t_end: float, window: float = 30.0, every: int = 4, num=None,
+               batched: bool = True) -> tuple:  # fmt: skip
+    """The storms on the catchment from dry ground to ``t_end``: each run's design-line peaks and their times (runs x
+    lines), its steps and its envelope, and the CUDA-event seconds around the runs. ``batched``: all runs in one batch
+    (the B200 form), else one plain run after another (the reference's order)."""
     import torch
 
     from wadi2d_b200.config import Numerics
 
     num = num or Numerics()
-    areas = [float(a) for a in areas]
-    check_study(storm, areas)
-    storms = storms_at(storm, areas)
-    n, nl = len(areas), len(cat.lines)
+    n, nl = len(storms), len(cat.lines)
     peaks, times = np.zeros((n, nl)), np.zeros((n, nl))
     steps = np.zeros(n, np.int64)
     envelopes: list[dict] = []
@@ -268,10 +263,61 @@ def run_study(cat, storm, areas, line_names, line_areas, cell_area, t_end: float
             del m, tally, maxima, lines_r, rain
         e1.record(stream)
         torch.cuda.synchronize()
-    seconds = e0.elapsed_time(e1) / 1e3
+    return peaks, times, steps, envelopes, e0.elapsed_time(e1) / 1e3
+
+
+def run_study(cat, storm, areas, line_names, line_areas, cell_area, t_end: float, window: float = 30.0,
+              every: int = 4, num=None, batched: bool = True, kind: str = "unspecified",
+              depth_floor: float | None = None) -> StudyResult:  # fmt: skip
+    """Every storm area of the study through the solver from dry ground to ``t_end``, then the design table and the
+    composites. ``cat``: the catchment (``critical.Catchment5``: grid, device tables, outfalls, outfall tally, rained
+    cells, design lines). ``batched``: all runs in one batch (the B200 form), else one plain run after another (the
+    reference's order). Seconds are CUDA-event time around the runs."""
+    areas = [float(a) for a in areas]
+    check_study(storm, areas)
+    peaks, times, steps, envelopes, seconds = solve_runs(cat, storms_at(storm, areas), t_end, window, every, num,
+                                                         batched)  # fmt: skip
     table = design_table(line_names, line_areas, areas, peaks, times, kind)
     composite = composite_maps(envelopes, areas, cell_area, depth_floor)
     return StudyResult(areas, peaks, times, table, composite, steps, seconds, envelopes)
+
+
+def run_study_sharded(cat, storm, areas, line_names, line_areas, cell_area, t_end: float, window: float = 30.0,
+                      every: int = 4, num=None, kind: str = "unspecified", depth_floor: float | None = None,
+                      world: int | None = None, rank: int | None = None, group=None,
+                      solve=None) -> StudyResult | None:  # fmt: skip
+    """The study over the ranks of a process group, one GPU a rank: the storm areas are split by ``sweep.partition``
+    (every run has the same catchment and end time, so the cost is equal), each rank solves its share as one batch,
+    and one gather (``sweep.gather_results``) brings every run's peaks, times, steps and envelope to rank 0, which
+    reads the design table and the composites. Returns the StudyResult on rank 0 (``seconds``: the slowest rank's),
+    None elsewhere. ``solve`` stands in for ``solve_runs`` (same arguments and results)."""
+    from wadi2d_b200.sweep import gather_results, partition
+
+    if world is None or rank is None:
+        import torch.distributed as dist
+
+        world, rank = dist.get_world_size(group), dist.get_rank(group)
+    areas = [float(a) for a in areas]
+    check_study(storm, areas)
+    storms = storms_at(storm, areas)
+    mine = partition([1.0] * len(areas), world)[rank]
+    local: dict = {}
+    if mine:
+        p, t, st, env, sec = (solve or solve_runs)(cat, [storms[i] for i in mine], t_end, window, every, num, True)
+        local = {i: (p[k], t[k], int(st[k]), env[k], sec) for k, i in enumerate(mine)}
+    merged = gather_results(local, world, rank, group)
+    if merged is None:
+        return None
+    if sorted(merged) != list(range(len(areas))):
+        raise ValueError("a storm area came back from no rank")
+    rec = [merged[i] for i in range(len(areas))]
+    peaks = np.stack([np.asarray(r[0], np.float64) for r in rec])
+    times = np.stack([np.asarray(r[1], np.float64) for r in rec])
+    steps = np.array([r[2] for r in rec], np.int64)
+    envelopes = [r[3] for r in rec]
+    table = design_table(line_names, line_areas, areas, peaks, times, kind)
+    composite = composite_maps(envelopes, areas, cell_area, depth_floor)
+    return StudyResult(areas, peaks, times, table, composite, steps, max(r[4] for r in rec), envelopes)
 
 
 def drainage_km2(cat) -> tuple[np.ndarray, np.ndarray]:

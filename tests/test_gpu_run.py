@@ -165,3 +165,37 @@ def test_design_lines_take_the_peak_discharge_every_step():
     qn = ln.discharge()
     xf, xs, yf, ys = lines[1]
     assert qn[1] == pytest.approx(float(np.dot(dev.read_cells("qx", xf), xs)), rel=1e-12)
+
+
+def test_fp64_level_in_the_near_dry_interval():
+    """Numerics.level_fp64: the level of a cell in its table's first interval is formed in FP64 (the row coordinate
+    and the interpolation), rounded once to float32; every other cell, and the depth, are as without it."""
+    w, og, g, tab = c1(64)
+    tables = GridTables.from_dict(g, tab)
+    rng = np.random.default_rng(4)
+    h0 = rng.uniform(0.0, 0.05, g.shape)  # shallow: many cells in their table's first interval
+
+    def one_step(fp64: bool):
+        m = Model(tables, Numerics(level_fp64=fp64))
+        m.stepper.adaptive_active = False
+        m.set_depth(h0)
+        m.run(1e9, max_steps=1)
+        return m.field("h"), m.field("d")
+
+    h_off, d_off = one_step(False)
+    h_on, d_on = one_step(True)
+    assert np.array_equal(h_on, h_off)
+    hc = g.from_tiles(tables.hc).astype(np.float32)
+    dtab = g.from_tiles(tables.dtab).astype(np.float32)
+    last = dtab.shape[-1] - 1
+    h = h_on.astype(np.float32)
+    inside = (hc > 0) & (h < hc)
+    with np.errstate(divide="ignore", invalid="ignore"):
+        s = np.sqrt(np.where(inside, h / np.where(hc > 0, hc, 1.0), 0.0).astype(np.float32)) * np.float32(last)
+    first = inside & (s.astype(np.int64) == 0)
+    assert first.sum() > 100
+    assert np.array_equal(d_on[~first], d_off[~first])
+    t0, t1 = dtab[..., 0].astype(np.float64), dtab[..., 1].astype(np.float64)
+    sd = np.sqrt(h.astype(np.float64) / np.where(hc > 0, hc, 1.0).astype(np.float64)) * float(last)
+    want = (t0 + sd * (t1 - t0)).astype(np.float32)
+    assert np.array_equal(d_on[first], want[first])

@@ -1,9 +1,9 @@
 """Exact solutions on the B200, as the reference's own analytic suite runs them (tests/solver/test_analytic.py:17-70,
 wadi2d/validation): the dam break on a wet bed (Stoker 1957) along x and along y, the dam break on a dry bed (Ritter
-1892), both on a flat frictionless bed, and still water over a seeded rough bed 1,500 m above the datum. The exact
-states are written here from the published formulas (as SWASHES gives them, Delestre et al. 2013); the limits are
-the reference's: depth and discharge RMSE over the cells wet in either field, the wet extent's F statistic, and the
-volume."""
+1892), both on a flat frictionless bed, Thacker's moving shoreline in a parabolic bowl (planar and curved, Thacker
+1981), and still water over a seeded rough bed 1,500 m above the datum. The exact states are written here from the
+published formulas (as SWASHES gives them, Delestre et al. 2013); the limits are the reference's: depth and discharge
+RMSE over the cells wet in either field, the wet extent's F statistic, and the volume."""
 
 from __future__ import annotations
 
@@ -163,3 +163,64 @@ def test_still_water_stays_still_on_rough_ground_at_altitude(sheet):
     assert np.abs(m.field("u"))[deep].max() < 1e-2
     assert np.abs(m.field("v"))[deep].max() < 1e-2
     assert abs(m.volume() / v0 - 1.0) < 1e-6
+
+
+def _thacker(kind: str):
+    """Thacker's oscillations in the bowl z = -h0 (1 - r^2 / a^2) (Thacker 1981, with SWASHES' parameters a = 1 m,
+    h0 = 0.1 m; the planar surface with eta = 0.5, the curved one with r0 = 0.8), frictionless, on 200 x 200 cells of
+    0.02 m with 4 x 4 pixels, started from the exact state averaged over each cell's pixels and run three periods."""
+    a, h0, n, dx, k = 1.0, 0.1, 200, 0.02, 4
+    xc = yc = 0.5 * n * dx
+
+    def bed(x, y):
+        return -h0 * (1.0 - ((x - xc) ** 2 + (y - yc) ** 2) / a**2)
+
+    if kind == "planar":
+        eta = 0.5
+        omega = math.sqrt(2.0 * G * h0) / a
+
+        def exact(x, y, t):
+            ph = omega * t
+            surface = eta * h0 / a**2 * (2.0 * (x - xc) * math.cos(ph) + 2.0 * (y - yc) * math.sin(ph) - eta)
+            h = np.maximum(surface - bed(x, y), 0.0)
+            return h, -eta * omega * math.sin(ph) * h, eta * omega * math.cos(ph) * h
+    else:
+        r0 = 0.8
+        amp = (a * a - r0 * r0) / (a * a + r0 * r0)
+        omega = math.sqrt(8.0 * G * h0) / a
+
+        def exact(x, y, t):
+            ph = omega * t
+            s = math.sqrt(1.0 - amp * amp) / (1.0 - amp * math.cos(ph))
+            rate = omega * amp * math.sin(ph) / (2.0 * (1.0 - amp * math.cos(ph)))
+            h = np.maximum(h0 * (s - ((x - xc) ** 2 + (y - yc) ** 2) / a**2 * s * s), 0.0)
+            return h, h * rate * (x - xc), h * rate * (y - yc)
+
+    m, tg, xs, ys, xcell, ycell = _model(n, n, dx, bed, k, 1e-6, PLAIN)
+    pny, pnx = tg.shape
+    hp, qxp, qyp = exact(xs, ys, 0.0)
+
+    def mean(f):
+        return np.broadcast_to(f, xs.shape).reshape(pny, k, pnx, k).mean(axis=(1, 3))
+
+    hbar, qx, qy = mean(hp), mean(qxp), mean(qyp)
+    inside = tg.mask
+    m.set_depth(np.where(inside, hbar, 0.0))
+    wet = hbar > 1e-9
+    m.set_velocity(np.where(wet & inside, qx / np.maximum(hbar, 1e-9), 0.0),
+                   np.where(wet & inside, qy / np.maximum(hbar, 1e-9), 0.0))  # fmt: skip
+    v0 = m.volume()
+    m.run(3.0 * 2.0 * math.pi / omega)
+    h, _, _ = _state(m, n, n, dx)
+    sl = (slice(PAD, PAD + n), slice(PAD, PAD + n))
+    he, _, _ = exact(xcell[sl], ycell[sl], m.stepper.t)
+    both = (h > WET) | (he > WET)
+    depth_rmse = float(np.sqrt(np.mean((h - he)[both] ** 2)))
+    return depth_rmse, m.volume() / v0 - 1.0
+
+
+@pytest.mark.parametrize("kind, limit", [("planar", 0.0055), ("curved", 0.002)])
+def test_thacker_moving_shoreline(kind, limit):
+    depth_rmse, volume = _thacker(kind)
+    assert depth_rmse < limit
+    assert abs(volume) < 5e-5

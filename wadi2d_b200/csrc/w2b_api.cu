@@ -23,7 +23,6 @@ int update_occupancy();
 void launch_update(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s);
 __global__ void boundary_kernel(StepArgs A, int control);
 __global__ void envelope_kernel(StepArgs A);
-__global__ void clock_kernel(StepArgs A);
 __global__ void control_kernel(StepArgs A);
 __global__ void prestep_kernel(StepArgs A);
 __global__ void setstep_kernel(StepArgs A, float dtf, int want_wave, int want_wet, int nact);

@@ -794,8 +794,6 @@ __device__ void run_clocks(const StepArgs& A) {
     }
 }
 
-__global__ void clock_kernel(StepArgs A) { run_clocks(A); }
-
 // Before a step of the device loop, for each run: the loop test and the step's settings
 // (wadi2d/solver/stepper.py:106-111). The threads of one CTA; ctl->any gathers the runs' flags.
 __device__ void step_settings(const StepArgs& A) {

@@ -222,13 +222,6 @@ class Batch:
             out[pl.oj * TILE : pl.oj * TILE + ny, pl.oi * TILE : pl.oi * TILE + nx] = np.where(g.mask, a, fill)
         return out
 
-    def _cut(self, r: int, a: np.ndarray) -> np.ndarray:
-        g, pl = self.grids[r], self.place[r]
-        ny, nx = g.shape
-        out = a[pl.oj * TILE : pl.oj * TILE + ny, pl.oi * TILE : pl.oi * TILE + nx].copy()
-        out[~g.mask] = 0.0
-        return out
-
     def halves(self) -> np.ndarray:
         """Each run's current half of the ping-pong pairs (h, u, v, mx, my)."""
         out = np.zeros(self.nruns, np.int32)

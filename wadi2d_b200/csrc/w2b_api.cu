@@ -723,10 +723,14 @@ static int loop_graph(Handle& H, int c) {
     int stc = W2B_OK;
     for (int k = 0; k < L.cand[c].steps && stc == W2B_OK; ++k) stc = launch_loop_step(H, L.cand[c], H.cap);
     cudaError_t e = cudaStreamEndCapture(H.cap, &graph);
-    if (stc != W2B_OK) return stc;
+    if (stc != W2B_OK) {
+        if (e == cudaSuccess) cudaGraphDestroy(graph);
+        return stc;
+    }
     CK(e);
     e = cudaGraphInstantiate(&L.exec[c], graph, 0);
     cudaGraphDestroy(graph);
+    if (e != cudaSuccess) L.exec[c] = nullptr;  // nothing to destroy later
     CK(e);
     L.version[c] = H.version;
     return W2B_OK;

@@ -17,8 +17,9 @@
  * the reference's void tile. Static per-cell and per-face arrays keep the reference's (ntiles, 32, 32) tile layout;
  * tables are repacked level-major (see w2b_pack_tables).
  *
- * Threading: one handle per stream; calls on one handle are not reentrant. The handle owns only host memory; every
- * device buffer is the caller's and must outlive the handle.
+ * Threading: one handle per stream; calls on one handle are not reentrant. The handle owns no device memory (only
+ * host memory, a capture stream, three events and the device loop's graphs, all released by w2b_destroy); every
+ * device buffer is the caller's and must outlive the handle. A call that fails returns no handle.
  */
 #ifndef WADI_B200_H
 #define WADI_B200_H

@@ -432,8 +432,13 @@ int32_t w2b_create(const W2BGridDesc* grid, const W2BParams* params, const W2BBu
         delete H;
         return cuda_status(cudaGetLastError(), "w2b_create events");
     }
+    const int st = cuda_status(cudaGetLastError(), "w2b_create");
+    if (st != W2B_OK) {  // no handle goes out with a failure: the caller has nothing to destroy
+        w2b_destroy(H);
+        return st;
+    }
     *handle = H;
-    return cuda_status(cudaGetLastError(), "w2b_create");
+    return W2B_OK;
 }
 
 int32_t w2b_destroy(void* handle) {

@@ -29,11 +29,10 @@ def test_library_exports_every_declared_symbol():
     assert len(names) >= 20
     missing = [n for n in names if not hasattr(lib, n)]
     assert not missing, missing
-    assert set(names) <= set(_lib._SIGNATURES) | {n for n in names if n.startswith("w2b_")}
 
 
-def test_every_bound_signature_is_declared():
-    assert set(_lib._SIGNATURES) <= set(declared())
+def test_every_declared_entry_point_is_bound_and_no_other():
+    assert set(_lib._SIGNATURES) == set(declared())
 
 
 def test_layout_and_index_conversion_match_python():
@@ -62,3 +61,18 @@ def test_bad_arguments_are_refused_without_a_gpu():
     ref = np.array([5], np.int64)  # an entry of the void tile
     out = np.zeros(1, np.int64)
     assert _lib.lib().w2b_ref_to_native(ctypes.byref(g), tiles.ctypes.data, 1, ref.ctypes.data, out.ctypes.data) == -1
+
+
+def test_every_entry_point_refuses_null_arguments_without_a_gpu():
+    """Every entry point checks its handle and pointers before it touches the device: called with null pointers and
+    zero sizes, each returns W2B_EINVAL (the sizing queries return their sizes)."""
+    sizes = {"w2b_version", "w2b_run_table_bytes", "w2b_table_workspace_doubles"}
+    L = _lib.lib()
+    for name, args in _lib._SIGNATURES.items():
+        if name in sizes:
+            continue
+        zeros = [0.0 if a in (ctypes.c_float, ctypes.c_double) else (0 if a in (ctypes.c_int32, ctypes.c_int64,
+                 ctypes.c_uint32) else None) for a in args]  # fmt: skip
+        assert getattr(L, name)(*zeros) == _lib.EINVAL, name
+    assert L.w2b_version() == 2
+    assert L.w2b_run_table_bytes(0) == 0

@@ -96,6 +96,8 @@ _SIGNATURES = {
     "w2b_tally": [c_vp, c_f64, c_vp],
     "w2b_advance": [c_vp, ctypes.POINTER(Stepper), c_f64, c_i64, ctypes.POINTER(Clock), c_vp],
     "w2b_build_tables": [c_vp, c_vp, c_vp],
+    "w2b_build_tables_noalloc": [c_vp, c_vp, c_vp],
+    "w2b_table_workspace_doubles": [c_i32, c_i64],
     "w2b_run_table_bytes": [c_i32],
     "w2b_set_run_dx": [c_vp, c_vp, c_i32],
     "w2b_run_halves": [c_vp, c_vp, c_vp],
@@ -117,6 +119,8 @@ _SIGNATURES = {
     "w2b_storage": [c_vp, c_i64, c_vp, c_vp, c_vp, c_vp],
 }
 
+_RETURNS_SIZE = ("w2b_run_table_bytes", "w2b_table_workspace_doubles")  # int64 sizes, not status codes
+
 _lib = None
 
 
@@ -133,7 +137,7 @@ def lib() -> ctypes.CDLL:
         for name, args in _SIGNATURES.items():
             fn = getattr(L, name)
             fn.argtypes = args
-            fn.restype = c_i64 if name == "w2b_run_table_bytes" else c_i32
+            fn.restype = c_i64 if name in _RETURNS_SIZE else c_i32
         _lib = L
     return _lib
 

@@ -39,8 +39,6 @@ class TableOut(ctypes.Structure):
 _L = _lib.lib()
 _L.w2b_build_tables.argtypes = [ctypes.POINTER(TableIn), ctypes.POINTER(TableOut), ctypes.c_void_p]
 _L.w2b_build_tables.restype = ctypes.c_int32
-_L.w2b_table_workspace_doubles.argtypes = [ctypes.c_int32, ctypes.c_int64]
-_L.w2b_table_workspace_doubles.restype = ctypes.c_int64
 
 
 class DeviceGridTables:

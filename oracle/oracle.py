@@ -21,7 +21,6 @@ Parity is pinned: ``tests/test_oracle_golden.py`` checks every array here bit fo
 from __future__ import annotations
 
 import ctypes
-import os
 import subprocess
 from dataclasses import dataclass, field
 from pathlib import Path

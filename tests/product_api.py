@@ -4,8 +4,6 @@
 
 from __future__ import annotations
 
-import numpy as np
-
 from oracle import oracle as O
 from wadi2d_b200 import tables as T
 from wadi2d_b200.backend import BoundaryCells

@@ -14,8 +14,8 @@ from wadi2d_b200.config import Numerics
 from wadi2d_b200.grid import TileGrid
 from wadi2d_b200.maxima import Tally
 from wadi2d_b200.model import Model
-from wadi2d_b200.run import DeviceRain, DeviceStorage, run_windows
-from wadi2d_b200.state import from_state, state_index
+from wadi2d_b200.run import DeviceRain, DeviceStorage
+from wadi2d_b200.state import state_index
 from wadi2d_b200.tables import GridTables
 
 pytestmark = pytest.mark.gpu

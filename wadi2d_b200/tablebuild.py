@@ -11,7 +11,6 @@ import numpy as np
 from wadi2d_b200 import _lib
 from wadi2d_b200.config import Tables
 from wadi2d_b200.grid import TileGrid
-from wadi2d_b200.layout import TILE2
 
 TILE_FIELDS = ("hc", "dtab", "efx", "efy", "ftabx", "ftaby", "zcx", "zcy", "flx", "frx", "glx", "grx", "cwx", "fly",
                "fry", "gly", "gry", "cwy")  # fmt: skip

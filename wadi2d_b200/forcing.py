@@ -225,13 +225,6 @@ class Injection:
         return weights / weights.sum()
 
 
-def triangular_hydrograph(peak: float, t_peak: float, base: float, n: int = 64) -> tuple[np.ndarray, np.ndarray]:
-    """Times and flows of a triangular unit-hydrograph shape: 0 at t = 0, ``peak`` at ``t_peak``, 0 at ``base``."""
-    times = np.array([0.0, t_peak, base])
-    flows = np.array([0.0, peak, 0.0])
-    return times, flows
-
-
 # ---------------------------------------------------------------------------------------------------- the window rate
 
 

@@ -99,16 +99,6 @@ class Catchment:
     initial_loss_mm: float
     constant_loss_mm_h: float
 
-    def rain_fraction(self, t: float) -> float:
-        """Cumulative share of the storm depth at time t: a triangular hyetograph peaking at half the storm."""
-        T = self.storm_s
-        if t <= 0.0:
-            return 0.0
-        if t >= T:
-            return 1.0
-        x = t / T
-        return 2.0 * x * x if x <= 0.5 else 1.0 - 2.0 * (1.0 - x) ** 2
-
     def boundary_cells(self) -> tuple[np.ndarray, np.ndarray]:
         rows = np.concatenate([r for r, _ in self.outfalls])
         cols = np.concatenate([c for _, c in self.outfalls])

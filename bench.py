@@ -145,6 +145,7 @@ def build_workload(n: int, device):
     c = workloads.catchment(n=n, device=device)
     grid = TileGrid.from_mask(np.ones((n, n), bool), 0.0, 0.0, c.dx)
     tables = build_tables(grid, ArrayBed(c.z, c.dx / c.k), Tables(), c.manning, device=device)
+    cut_block(c, grid)
     del c.z
     m = Model(tables, Numerics())
     m.stepper.adaptive_active = False
@@ -154,9 +155,7 @@ def build_workload(n: int, device):
     m.set_boundary(BoundaryCells(cells, cells.copy(), np.ones(nb, np.int32), np.zeros(nb, np.float32),
                                  np.zeros(nb, np.float32)))  # fmt: skip
     m.set_depth(np.where(grid.mask, 0.05, 0.0))
-    # rain excess at the hyetograph's peak (2 D / T), less the constant loss, m/s
-    peak_mm_h = 2.0 * c.rain_mm / (c.storm_s / 3600.0)
-    rate = np.maximum(peak_mm_h - c.constant_loss_mm_h, 0.0) / 3.6e6
+    rate = peak_rate(c)
     m.set_source(np.where(grid.mask, rate, 0.0))
     # outflow faces of the outfall cells (east/south faces of the rim cells are their own west/north faces)
     maxima = Maxima(m, 0.1, 0.05, every=4)
@@ -164,31 +163,44 @@ def build_workload(n: int, device):
     return m, c, grid, tables, maxima, tally, rate
 
 
-def cpu_sample(tables, grid, rate, seconds: float, threads: int, steps: int | None = None, warmup: int = 1):
-    """The oracle on a 32 x 32-tile block cut from the middle of the workload: cell-steps/s on ``threads`` host
-    threads, over about ``seconds`` (or exactly ``steps``) of stepping."""
-    from oracle import oracle as O
+def peak_rate(c) -> np.ndarray:
+    """Rain excess at the hyetograph's peak (2 D / T), less the constant loss, m/s, on the padded grid."""
+    peak_mm_h = 2.0 * c.rain_mm / (c.storm_s / 3600.0)
+    return np.maximum(peak_mm_h - c.constant_loss_mm_h, 0.0) / 3.6e6
 
-    O.threads(threads)
+
+def cut_block(c, grid) -> None:
+    """Keep the CPU sample block's pixels, with the one-pixel rim the table builder reads, on the host
+    (``c.block_z``)."""
+    j0, i0, M = cpu_block(grid)
+    c.block_z = c.z[j0 * c.k : (j0 + M) * c.k + 2, i0 * c.k : (i0 + M) * c.k + 2].double().cpu().numpy()
+
+
+def cpu_block(grid) -> tuple[int, int, int]:
+    """First row and column (padded cells) and side of the CPU sample: a 32 x 32-tile block from the middle of the
+    grid."""
     B = CPU_BLOCK_TILES
     nty, ntx = grid.tile_of.shape
-    tj0, ti0 = (nty - B) // 2, (ntx - B) // 2
-    ids = grid.tile_of[tj0 : tj0 + B, ti0 : ti0 + B].reshape(-1)
-    mask = np.ones((B * 32, B * 32), bool)
-    og = O.Grid(0.0, 0.0, grid.dx, mask)
-    order = ids[(og.tiles[1:, 0]) * B + og.tiles[1:, 1]]
-    dev = tables.device_arrays
-    import torch
+    return (nty - B) // 2 * 32, (ntx - B) // 2 * 32, B * 32
 
-    sel = torch.as_tensor(np.concatenate(([0], order)), device=dev["hc"].device)
-    sub = {n: dev[n].index_select(0, sel).cpu().numpy() for n in dev if n not in ("zmin", "zbar")}
-    sub["rows"] = tables.rows
-    sub["zmin"] = np.zeros(mask.shape)
-    m = O.Model(og, sub, O.Numerics())
+
+def cpu_sample(c, grid, rate, seconds: float, threads: int, steps: int | None = None, warmup: int = 1):
+    """The oracle on the CPU sample block of the workload, as the reference's CPU path would take it: the block's
+    pixels (``c.block_z``, cut from the catchment's bed), tables built from them by the oracle's table builder (the
+    reference's builder restated; faces at the block's edge see the block's own pixels), the source rates of the
+    block's cells, 0.05 m of water everywhere. Returns cell-steps/s on ``threads`` host threads over about
+    ``seconds`` (or exactly ``steps``) of stepping, the steps, the seconds and the cells."""
+    from oracle import oracle as O
+
+    j0, i0, M = cpu_block(grid)
+    mask = np.ones((M, M), bool)
+    og = O.Grid(0.0, 0.0, grid.dx, mask)
+    tables = O.build_tables(og, c.block_z, c.dx / c.k, c.manning, local_radius=True)
+    O.threads(threads)
+    m = O.Model(og, tables, O.Numerics())
     m.adaptive_active = False
     m.set_depth(np.full(mask.shape, 0.05))
-    r = rate[tj0 * 32 : (tj0 + B) * 32, ti0 * 32 : (ti0 + B) * 32]
-    m.set_source(r)
+    m.set_source(rate[j0 : j0 + M, i0 : i0 + M])
     cells = mask.size
     for _ in range(warmup):
         m.advance(m.t + m.dt * 0.999)
@@ -209,10 +221,16 @@ def run_reference(args) -> None:
         return
     import torch
 
+    from wadi2d_b200 import workloads
+    from wadi2d_b200.grid import TileGrid
+
     threads = os.cpu_count() or 1
     dev = torch.device("cuda", 0) if torch.cuda.is_available() else torch.device("cpu")
-    _, _, grid, tables, _, _, rate = build_workload(args.n, dev)
-    value, done, el, cells = cpu_sample(tables, grid, rate, 0.0, threads, steps=args.steps, warmup=args.warmup)
+    c = workloads.catchment(n=args.n, device=dev)  # the seeded bed, generated with torch
+    grid = TileGrid.from_mask(np.ones((args.n, args.n), bool), 0.0, 0.0, c.dx)
+    cut_block(c, grid)
+    del c.z
+    value, done, el, cells = cpu_sample(c, grid, peak_rate(c), 0.0, threads, steps=args.steps, warmup=args.warmup)
     sample = f"{CPU_BLOCK_TILES}x{CPU_BLOCK_TILES} tiles ({cells} cells) of the workload, {done} steps"
     line = {
         "impl": "reference", "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": args.gpus,
@@ -815,7 +833,7 @@ def main() -> None:
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        cv, done, el, ccells = cpu_sample(tables, grid, rate, args.cpu_seconds, threads)
+        cv, done, el, ccells = cpu_sample(c, grid, rate, args.cpu_seconds, threads)
         cpu = {"value": cv, "unit": "cell-steps/s", "cores": threads, "kind": "port",
                "sample": f"{CPU_BLOCK_TILES}x{CPU_BLOCK_TILES} tiles ({ccells} cells) of the workload, {done} steps "
                          f"in {el:.1f} s"}  # fmt: skip
@@ -830,7 +848,8 @@ def main() -> None:
             "config": {"workload": f"configuration 3: {args.n}x{args.n} cells at 30 m, 4x4 pixels, wet start under peak "
                                    "rain, every tile stepped, envelope every 4 steps, FP64 tally every step",
                        "cells": cells, "tiles": grid.ntiles - 1, "wet_fraction": wet, "cfl": m.num.cfl,
-                       "l2": "inputs larger than L2 (about 15 GB resident)", "parallelism": f"replicas x{world}",
+                       "l2": f"inputs larger than L2 ({torch.cuda.memory_allocated(dev) / 1e9:.1f} GB resident)",
+                       "parallelism": f"replicas x{world}",
                        "loop": "device-resident, CUDA graphs", "launch": b.loop_config(),
                        "tuning_steps": tune_steps},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,

@@ -137,6 +137,12 @@ int64_t w2b_run_table_bytes(int32_t nruns);
  * cbrt is formed. out (device, 5 uint64, zeroed by the caller): [0] mismatches, [1..4] some mismatching inputs. */
 int32_t w2b_selftest_cbrt(uint32_t first_bits, uint32_t count, uint64_t* out, void* stream);
 
+/* Self-check of the bounded device wait (no counterpart in the reference): a barrier that nothing completes, waited on
+ * for polls polls (1 <= polls <= 262144, the limit every wait of the library uses) by the library's own wait. out
+ * (device, 2 int64): [0] the status the wait reports, W2B_ETIMEOUT when it gives up, as it must; [1] the SM clock
+ * cycles it took. The context stays usable afterwards. */
+int32_t w2b_selftest_wait(uint32_t polls, int64_t* out, void* stream);
+
 /* Native layout of a grid. */
 int32_t w2b_layout(const W2BGridDesc* grid, W2BLayout* out);
 

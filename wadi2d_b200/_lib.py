@@ -75,6 +75,7 @@ class Clock(ctypes.Structure):
 _SIGNATURES = {
     "w2b_version": [],
     "w2b_selftest_cbrt": [ctypes.c_uint32, ctypes.c_uint32, c_vp, c_vp],
+    "w2b_selftest_wait": [ctypes.c_uint32, c_vp, c_vp],
     "w2b_layout": [ctypes.POINTER(GridDesc), ctypes.POINTER(Layout)],
     "w2b_ref_to_native": [ctypes.POINTER(GridDesc), c_vp, c_i64, c_vp, c_vp],
     "w2b_create": [ctypes.POINTER(GridDesc), ctypes.POINTER(Params), ctypes.POINTER(Buffers), ctypes.POINTER(c_vp)],

@@ -11,11 +11,13 @@
 #include <cuda.h>
 
 #include "w2b_common.cuh"
+#include "w2b_tma.cuh"
 
 namespace w2b {
 cudaError_t faces_setup();
 void launch_probe(const StepArgs& A, int t, float dt, float* out, cudaStream_t s);
 void launch_cbrt_check(uint32_t first, uint32_t count, unsigned long long* out, cudaStream_t s);
+void launch_wait_check(uint32_t polls, long long* out, cudaStream_t s);
 int faces_occupancy();
 void launch_faces(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s);
 cudaError_t update_setup();
@@ -338,6 +340,13 @@ int32_t w2b_selftest_cbrt(uint32_t first_bits, uint32_t count, uint64_t* out, vo
     if (!out) return W2B_EINVAL;
     launch_cbrt_check(first_bits, count, reinterpret_cast<unsigned long long*>(out), (cudaStream_t)stream);
     CKL("w2b_selftest_cbrt");
+    return W2B_OK;
+}
+
+int32_t w2b_selftest_wait(uint32_t polls, int64_t* out, void* stream) {
+    if (!out || polls < 1 || polls > TMA_WAIT_LIMIT) return W2B_EINVAL;
+    launch_wait_check(polls, reinterpret_cast<long long*>(out), (cudaStream_t)stream);
+    CKL("w2b_selftest_wait");
     return W2B_OK;
 }
 

@@ -391,6 +391,24 @@ void launch_cbrt_check(uint32_t first, uint32_t count, unsigned long long* out, 
     cbrt_check_kernel<<<148 * 16, 256, 0, s>>>(first, count, out);
 }
 
+// The bounded wait's give-up path, run on purpose: thread 0 arms a barrier for 16 bytes that no copy will bring, so
+// its phase cannot complete, and waits on it with mbar_wait for `polls` polls. Nothing is in flight, so the CTA may
+// leave. out[0] = W2B_ETIMEOUT if the wait gave up (W2B_OK if it completed, which it cannot), out[1] = the clock
+// cycles the wait took.
+__global__ void wait_check_kernel(uint32_t polls, long long* out) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+    mbar_expect_tx(&bar, 16);  // the one arrival, with 16 bytes still expected
+    const long long t0 = clock64();
+    const bool ok = mbar_wait(&bar, 0, polls);
+    out[1] = clock64() - t0;
+    out[0] = ok ? W2B_OK : W2B_ETIMEOUT;
+}
+
+void launch_wait_check(uint32_t polls, long long* out, cudaStream_t s) { wait_check_kernel<<<1, 32, 0, s>>>(polls, out); }
+
 // The wave speed and the new velocity of every own face of tile t for a step dt from the current state, as the face
 // pass would compute them, written to out ([wx | wy | un_x | un_y], 1024 each, tile layout) and nothing else: the
 // device side of the step limiter (wadi2d/solver/limiter.py:31-55, the CPU twin's face_step on one tile). One CTA;

@@ -8,7 +8,7 @@
 
 namespace w2b {
 
-constexpr uint32_t TMA_WAIT_LIMIT = 1u << 22;
+constexpr uint32_t TMA_WAIT_LIMIT = 1u << 18;  // about 1 s: a poll that finds the phase open takes about 4 us
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -41,9 +41,10 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t phase) {
     return ok != 0;
 }
 
-// Wait for the barrier's phase; false if the wait gave up.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase) {
-    for (uint32_t it = 0; it < TMA_WAIT_LIMIT; ++it)
+// Wait for the barrier's phase; false if the wait gave up (after `limit` polls: TMA_WAIT_LIMIT everywhere but in the
+// wait's own self-check).
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t phase, uint32_t limit = TMA_WAIT_LIMIT) {
+    for (uint32_t it = 0; it < limit; ++it)
         if (mbar_try_wait(bar, phase)) return true;
     return false;
 }

@@ -1,6 +1,6 @@
 // Tensor Memory Accelerator helpers for sm_100a: mbarrier, 2D tiled and 1D bulk copies global -> shared memory.
-// Every wait is bounded: after TMA_WAIT_LIMIT polls the caller gives up and reports W2B_ETIMEOUT. No copy here uses
-// cluster multicast: every source is this GPU's own memory, read by the CTA that needs it.
+// Every wait is bounded: after TMA_WAIT_LIMIT polls the caller gives up and reports W2B_ETIMEOUT. Every copy here
+// lands in the shared memory of the one CTA that issues it, from this GPU's own memory.
 #pragma once
 
 #include <cuda.h>

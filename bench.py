@@ -42,6 +42,11 @@ sys.path.insert(0, str(ROOT))
 ALG_STEP = 194.0
 ALG_FACES = 32.0 + 0.5 + 8.0 + 48.0 + 32.0 + 24.0
 FALLBACK_HBM_GBS = 6650.0
+# DRAM bytes a tile cell of the face pass (dram__bytes_read.sum + dram__bytes_write.sum of one launch, divided by the
+# launch's tile cells), from an ncu capture of faces_kernel on configuration 3's catchment at 1024 x 1024 cells
+# (1,115,136 tile cells, beyond L2); the traffic grows with the tile cells a launch processes, so it scales to this
+# launch by them.
+FACES_DRAM_BYTES_PER_CELL = 178.6
 CPU_BLOCK_TILES = 32  # the CPU sample: a 32 x 32-tile block (1,048,576 cells) from the middle of the grid
 
 
@@ -51,6 +56,11 @@ def parse():
     p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=("b200", "reference"))
+    p.add_argument("--arith", default="exact", choices=("exact", "fast"),
+                   help="the step's build: exact (the reference's float32 bits) or fast (FMA contraction, approximate "
+                        "division, square root and cube root in the face pass)")
+    p.add_argument("--parity-steps", type=int, default=200,
+                   help="steps of the CUDA path against the oracle on the CPU sample block (0: none)")
     p.add_argument("--n", type=int, default=4096, help="domain side in cells (configuration 3: 4096)")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
@@ -71,6 +81,9 @@ def parse():
     p.add_argument("--study-n", type=int, default=1024, help="--arf-study: catchment cells a side")
     p.add_argument("--config2-run", action="store_true",
                    help="configuration 2 end to end: 1024 x 1024, crests, lumped inflows, a reservoir, 6 h")
+    p.add_argument("--host-inflows", action="store_true",
+                   help="--config2-run: share the inflows on the host (levels read back each window, the window's "
+                        "source uploaded) instead of on the device")
     p.add_argument("--table-build", action="store_true",
                    help="the GPU table build of configuration 2 (1024 x 1024, 1 m pixels) and 3 (4096 x 4096, 7.5 m)")
     p.add_argument("--critical", action="store_true",
@@ -78,6 +91,10 @@ def parse():
     p.add_argument("--candidates", type=int, default=400, help="--critical: candidate storms")
     p.add_argument("--train-runs", type=int, default=96, help="--critical: solver runs the network learns from")
     p.add_argument("--plain-sample", type=int, default=8, help="--critical: runs timed one after another")
+    p.add_argument("--critical-dx", type=float, default=10.0, help="--critical: cell size, m")
+    p.add_argument("--critical-relief", type=float, default=None,
+                   help="--critical: relief of the catchment, m (default 3 %% of its length)")
+    p.add_argument("--no-sweep", action="store_true", help="leave the bounded storm sweep out of the default line")
     return p.parse_args()
 
 
@@ -132,7 +149,7 @@ class Clocks:
                 "reasons": sorted(reasons), "samples": len(sm)}  # fmt: skip
 
 
-def build_workload(n: int, device):
+def build_workload(n: int, device, arith: str = "exact"):
     """Configuration 3 on the GPU: catchment, tables, model, outfalls, wet start under peak rain."""
     from wadi2d_b200 import workloads
     from wadi2d_b200.backend import BoundaryCells
@@ -147,7 +164,7 @@ def build_workload(n: int, device):
     tables = build_tables(grid, ArrayBed(c.z, c.dx / c.k), Tables(), c.manning, device=device)
     cut_block(c, grid)
     del c.z
-    m = Model(tables, Numerics())
+    m = Model(tables, Numerics(arithmetic=arith))
     m.stepper.adaptive_active = False
     rows, cols = c.boundary_cells()
     cells = np.array([m.cell_state_index(int(j), int(i)) for j, i in zip(rows, cols, strict=True)], np.int32)
@@ -184,24 +201,32 @@ def cpu_block(grid) -> tuple[int, int, int]:
     return (nty - B) // 2 * 32, (ntx - B) // 2 * 32, B * 32
 
 
-def cpu_sample(c, grid, rate, seconds: float, threads: int, steps: int | None = None, warmup: int = 1):
-    """The oracle on the CPU sample block of the workload, as the reference's CPU path would take it: the block's
-    pixels (``c.block_z``, cut from the catchment's bed), tables built from them by the oracle's table builder (the
-    reference's builder restated; faces at the block's edge see the block's own pixels), the source rates of the
-    block's cells, 0.05 m of water everywhere. Returns cell-steps/s on ``threads`` host threads over about
-    ``seconds`` (or exactly ``steps``) of stepping, the steps, the seconds and the cells."""
+def block_inputs(c, grid, rate):
+    """The CPU sample block as the reference's CPU path takes it: the oracle's grid of the block (every cell active,
+    walls on its edge), its tables from the oracle's table builder (the reference's builder restated) on the block's
+    own pixels (``c.block_z``, cut from the catchment's bed; faces at the block's edge see the block's pixels), and the
+    source rates of the block's cells."""
     from oracle import oracle as O
 
     j0, i0, M = cpu_block(grid)
-    mask = np.ones((M, M), bool)
-    og = O.Grid(0.0, 0.0, grid.dx, mask)
+    og = O.Grid(0.0, 0.0, grid.dx, np.ones((M, M), bool))
     tables = O.build_tables(og, c.block_z, c.dx / c.k, c.manning, local_radius=True)
+    return og, tables, rate[j0 : j0 + M, i0 : i0 + M]
+
+
+def cpu_sample(block, seconds: float, threads: int, steps: int | None = None, warmup: int = 1):
+    """The oracle on the CPU sample block (``block_inputs``), 0.05 m of water everywhere under the block's rates.
+    Returns cell-steps/s on ``threads`` host threads over about ``seconds`` (or exactly ``steps``) of stepping, the
+    steps, the seconds and the cells."""
+    from oracle import oracle as O
+
+    og, tables, rate = block
     O.threads(threads)
     m = O.Model(og, tables, O.Numerics())
     m.adaptive_active = False
-    m.set_depth(np.full(mask.shape, 0.05))
-    m.set_source(rate[j0 : j0 + M, i0 : i0 + M])
-    cells = mask.size
+    m.set_depth(np.full(og.mask.shape, 0.05))
+    m.set_source(rate)
+    cells = og.mask.size
     for _ in range(warmup):
         m.advance(m.t + m.dt * 0.999)
     n0, t0 = m.nsteps, time.perf_counter()
@@ -212,6 +237,74 @@ def cpu_sample(c, grid, rate, seconds: float, threads: int, steps: int | None = 
         if (steps is not None and done >= steps) or (steps is None and el >= seconds and done >= 3):
             break
     return cells * done / el, done, el, cells
+
+
+class _Stop(Exception):
+    pass
+
+
+def _steps(model, n: int) -> None:
+    """n steps of a model's host-driven loop (the reference's Stepper.advance, dt rule and refresh cadence)."""
+
+    def cb(st):
+        if st.nsteps >= n:
+            raise _Stop
+
+    try:
+        model.advance(1e12, cb)
+    except _Stop:
+        pass
+
+
+def block_parity(block, arith: str, steps: int, threads: int) -> dict:
+    """The CUDA step against the oracle on the CPU sample block: the same tables (the oracle's), 0.05 m of water under
+    the block's peak rain, ``steps`` steps of each's host-driven loop at the reference's dt rule, then the step's
+    accuracy bounds: the dt sequence, the wet set (h > 0), depth within 1e-5 m or 1e-4 relative, unit discharge within
+    1e-4 of its field's scale; and whether every state field is equal bit for bit."""
+    from oracle import oracle as O
+    from wadi2d_b200.config import Numerics
+    from wadi2d_b200.grid import TileGrid
+    from wadi2d_b200.model import Model
+    from wadi2d_b200.tables import GridTables
+
+    og, tables, rate = block
+    O.threads(threads)
+    ref = O.Model(og, tables, O.Numerics())
+    ref.adaptive_active = False
+    grid = TileGrid(0.0, 0.0, og.dx, og.mask)
+    m = Model(GridTables.from_dict(grid, tables), Numerics(arithmetic=arith))
+    m.stepper.adaptive_active = False
+    dts = []
+    step = m.backend.step
+
+    def logged(dt, want_wave, want_wet):
+        dts.append(float(dt))
+        step(dt, want_wave, want_wet)
+
+    m.backend.step = logged
+    for model in (ref, m):
+        model.set_depth(np.full(og.mask.shape, 0.05))
+        model.set_source(rate)
+        _steps(model, steps)
+    out = {"arith": arith, "steps": int(m.stepper.nsteps), "cells": int(og.mask.size),
+           "dt_identical": dts == [float(x) for x in ref.dts],
+           "dt_max_rel_diff": float(np.max(np.abs(np.array(dts) / np.array(ref.dts) - 1.0))) if dts else 0.0}  # fmt: skip
+    f = {n: (m.field(n), ref.field(n)) for n in ("h", "d", "u", "v", "mx", "my", "qx", "qy", "res", "om")}
+    out["bit_identical"] = all(np.array_equal(a, b) for a, b in f.values())
+    h, hr = (x.astype(np.float64) for x in f["h"])
+    diff = np.abs(h - hr)
+    out["wet_set_identical"] = bool(np.array_equal(h > 0, hr > 0))
+    out["depth_max_abs_err_m"] = float(diff.max())
+    out["depth_within"] = bool(np.all((diff <= 1e-5) | (diff <= 1e-4 * np.abs(hr))))
+    rel = {}
+    for n in ("qx", "qy", "u", "v", "d"):
+        a, b = (x.astype(np.float64) for x in f[n])
+        rel[n] = float(np.abs(a - b).max() / max(np.abs(b).max(), 1e-30))
+    out["rel_to_scale"] = rel
+    out["discharge_within"] = rel["qx"] <= 1e-4 and rel["qy"] <= 1e-4
+    out["within_bounds"] = out["wet_set_identical"] and out["depth_within"] and out["discharge_within"]
+    del m
+    return out
 
 
 def run_reference(args) -> None:
@@ -230,7 +323,8 @@ def run_reference(args) -> None:
     grid = TileGrid.from_mask(np.ones((args.n, args.n), bool), 0.0, 0.0, c.dx)
     cut_block(c, grid)
     del c.z
-    value, done, el, cells = cpu_sample(c, grid, peak_rate(c), 0.0, threads, steps=args.steps, warmup=args.warmup)
+    block = block_inputs(c, grid, peak_rate(c))
+    value, done, el, cells = cpu_sample(block, 0.0, threads, steps=args.steps, warmup=args.warmup)
     sample = f"{CPU_BLOCK_TILES}x{CPU_BLOCK_TILES} tiles ({cells} cells) of the workload, {done} steps"
     line = {
         "impl": "reference", "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": args.gpus,
@@ -447,14 +541,17 @@ def ensemble_run(args) -> None:
         dist.destroy_process_group()
 
 
-def critical_run(args) -> None:
-    """Configuration 5 at args.n cells (256 by default; the configuration names 1024): which of args.candidates storms
-    (0.5-48 h log-uniform, 20-200 mm, ARF 0.6-1.0, patterns a seeded convex mix of 4 alternating-block hyetographs)
-    gives the largest peak flow at the main design point. Three ways, timed with CUDA events: every candidate through
-    the solver as batches (the exhaustive sweep), the network's screen (solver runs of args.train_runs candidates,
-    training, ranking, solver runs of the top 5 %), and one solver run after another on a sample of args.plain_sample
-    candidates, whose time per simulated hour gives the one-after-another sweep's runs/h. A non-learned screen (the
-    same share ranked by peak block intensity) shows what the network adds."""
+def critical_search(n: int, candidates: int, train_runs: int, plain_sample: int, dx: float = 10.0,
+                    relief: float | None = None, seed: int = 17, storm_seed: int = 5, iters: int = 3000,
+                    arith: str = "exact") -> dict:
+    """Configuration 5 on an n x n catchment at dx (relief by default 3 % of its length): which of ``candidates``
+    storms (0.5-48 h log-uniform, 20-200 mm, ARF 0.6-1.0, patterns a seeded convex mix of 4 alternating-block
+    hyetographs) gives the largest peak flow at the main design point. Three ways, timed with CUDA events: every
+    candidate through the solver as batches (the exhaustive sweep), the network's screen (solver runs of
+    ``train_runs`` candidates, training, ranking, solver runs of the top 5 %), and one solver run after another on a
+    sample of ``plain_sample`` candidates, whose time per simulated hour gives the one-after-another sweep's runs/h.
+    A non-learned screen (the same share ranked by peak block intensity, with the same training runs) shows what the
+    network adds."""
     import torch
 
     from wadi2d_b200 import critical as C
@@ -475,24 +572,24 @@ def critical_run(args) -> None:
         torch.cuda.synchronize(dev)
         return out, e0.elapsed_time(e1) / 1e3
 
-    n = args.n if args.n != 4096 else 256
+    num = Numerics(arithmetic=arith)
     t0 = time.perf_counter()
-    cat = C.prepare(n=n, dx=10.0, k=4, seed=17, device=dev)
+    cat = C.prepare(n=n, dx=dx, k=4, seed=seed, relief=relief, device=dev)
     setup = time.perf_counter() - t0
-    storms = C.candidates(args.candidates, seed=5)
+    storms = C.candidates(candidates, seed=storm_seed)
     x = C.features(storms)
     rec = 1.0
     sim_h = np.array([s.duration_h + rec for s in storms])
-    full, full_s = timed(lambda: C.solve(cat, storms, recession_h=rec))
+    full, full_s = timed(lambda: C.solve(cat, storms, recession_h=rec, num=num))
     point = 0
     crit = int(np.argmax(full["peak_q"][:, point]))
     rng = np.random.default_rng(11)
-    train = rng.choice(len(storms), size=args.train_runs, replace=False)
-    res_tr, tr_s = timed(lambda: C.solve(cat, [storms[i] for i in train], recession_h=rec))
+    train = rng.choice(len(storms), size=train_runs, replace=False)
+    res_tr, tr_s = timed(lambda: C.solve(cat, [storms[i] for i in train], recession_h=rec, num=num))
     y_tr = C.targets(res_tr)
-    (order, pred, losses), fit_s = timed(lambda: C.screen(x[train], y_tr, x, top=0.05, point=point, iters=3000))
+    (order, pred, losses), fit_s = timed(lambda: C.screen(x[train], y_tr, x, top=0.05, point=point, iters=iters))
     rerun = [int(i) for i in order if i not in set(train.tolist())]
-    res_rr, rr_s = timed(lambda: C.solve(cat, [storms[i] for i in rerun], recession_h=rec) if rerun else None)
+    res_rr, rr_s = timed(lambda: C.solve(cat, [storms[i] for i in rerun], recession_h=rec, num=num) if rerun else None)
     solved = {int(i): float(res_tr["peak_q"][k, point]) for k, i in enumerate(train)}
     for k, i in enumerate(rerun):
         solved[i] = float(res_rr["peak_q"][k, point])
@@ -500,18 +597,19 @@ def critical_run(args) -> None:
     screen_s = tr_s + fit_s + rr_s
     # the same share ranked without the network: by the storm's peak block intensity (descriptor 9)
     k = len(order)
-    naive = set(np.argsort(x[:, 9])[::-1][:k].tolist()) | set(train.tolist())
+    by_intensity = np.argsort(x[:, 9])[::-1][:k]
+    naive = set(by_intensity.tolist()) | set(train.tolist())
     naive_found = max(naive, key=lambda i: full["peak_q"][i, point])
     held = np.setdiff1d(np.arange(len(storms)), train)
     truth = np.log1p(full["peak_q"][held, point])
     r2 = 1.0 - np.mean((pred[held, point] - truth) ** 2) / np.var(truth)
     # one run after another, on a sample
-    sample = rng.choice(len(storms), size=args.plain_sample, replace=False)
+    sample = rng.choice(len(storms), size=plain_sample, replace=False)
 
     def plain():
         out = []
         for i in sample:
-            m = Model(cat.tables, Numerics())
+            m = Model(cat.tables, num)
             m.set_boundary(cat.boundary)
             m.set_depth(np.zeros(cat.grid.shape))
             tally = Tally(m, *cat.tally)
@@ -525,26 +623,37 @@ def critical_run(args) -> None:
     same = all(plain_q[j] == full["peak_q"][i, point] for j, i in enumerate(sample))
     plain_per_h = plain_s / sim_h[sample].sum()  # seconds of one-after-another solving per simulated hour
     plain_sweep_s = plain_per_h * sim_h.sum()
-    line = {
-        "run": "configuration 5 critical-duration search", "cells": n * n, "dx_m": 10.0,
-        "candidates": len(storms), "design_points": len(cat.lines), "train_runs": int(args.train_runs),
-        "rerun_top": len(rerun), "setup_s": setup,
+    return {
+        "run": "configuration 5 critical-duration search", "cells": n * n, "dx_m": dx, "relief_m": cat.relief,
+        "arith": arith, "candidates": len(storms), "design_points": len(cat.lines), "train_runs": int(train_runs),
+        "top": k, "rerun_top": len(rerun), "setup_s": setup,
+        "critical_in_training_runs": bool(crit in set(train.tolist())),
         "exhaustive_batched": {"s": full_s, "runs_per_h": 3600.0 * len(storms) / full_s,
                                "critical": crit, "peak_q": float(full["peak_q"][crit, point]),
-                               "duration_h": storms[crit].duration_h},
+                               "duration_h": storms[crit].duration_h, "depth_mm": storms[crit].total_depth},
         "screened": {"s": screen_s, "solver_s": tr_s + rr_s, "train_s": fit_s,
                      "runs_per_h": 3600.0 * len(storms) / screen_s, "critical": found,
                      "peak_q": solved[found], "same_critical": found == crit,
+                     "critical_in_top": bool(crit in set(order.tolist())),
                      "peak_q_error": solved[found] / float(full["peak_q"][crit, point]) - 1.0,
                      "held_out_r2_log_peak": float(r2), "loss_first_last": [losses[0], losses[-1]]},
-        "naive_screen": {"critical": int(naive_found), "same_critical": int(naive_found) == crit,
-                         "peak_q_error": float(full["peak_q"][naive_found, point] / full["peak_q"][crit, point]) - 1.0},
+        "intensity_screen": {"critical": int(naive_found), "same_critical": int(naive_found) == crit,
+                             "critical_in_top": bool(crit in set(by_intensity.tolist())),
+                             "peak_q_error": float(full["peak_q"][naive_found, point] / full["peak_q"][crit, point])
+                             - 1.0},
         "plain_one_after_another": {"sample": len(sample), "s_sample": plain_s, "s_per_simulated_h": plain_per_h,
                                     "sweep_s_estimate": plain_sweep_s,
                                     "runs_per_h": 3600.0 * len(storms) / plain_sweep_s, "same_peaks_as_batch": same},
         "speedup_screened_vs_plain": plain_sweep_s / screen_s,
         "speedup_batched_vs_plain": plain_sweep_s / full_s,
     }  # fmt: skip
+
+
+def critical_run(args) -> None:
+    """``critical_search`` at the command line's sizes (256 x 256 cells by default; the configuration names 1024)."""
+    n = args.n if args.n != 4096 else 256
+    line = critical_search(n, args.candidates, args.train_runs, args.plain_sample, dx=args.critical_dx,
+                           relief=args.critical_relief, arith=args.arith)  # fmt: skip
     print(json.dumps(line), flush=True)
 
 
@@ -563,7 +672,7 @@ def config2_run(args) -> None:
     from wadi2d_b200.grid import TileGrid
     from wadi2d_b200.maxima import Maxima, Tally
     from wadi2d_b200.model import Model
-    from wadi2d_b200.run import DeviceStorage, run_windows
+    from wadi2d_b200.run import DeviceInflow, DeviceStorage, run_windows
     from wadi2d_b200.state import state_index
     from wadi2d_b200.tables import ArrayBed, build_tables, hbar_at_level
 
@@ -601,13 +710,17 @@ def config2_run(args) -> None:
         idx = state_index(grid, ir, icol).astype(np.int64)
         injections.append(F.Injection(f"inflow {q}", np.array([pos[int(k)] for k in idx]), idx, low, times, flows,
                                       0.1))  # fmt: skip
-    forcing = F.Forcing(interior, c.dx**2, injections=injections,
-                        depth_reader=lambda inj: m.read_cells("d", inj.index))  # fmt: skip
     storage = DeviceStorage(m, interior)
+    if args.host_inflows:
+        forcing = F.Forcing(interior, c.dx**2, injections=injections,
+                            depth_reader=lambda inj: m.read_cells("d", inj.index))  # fmt: skip
+        sources = {"host_forcing": forcing}
+    else:
+        sources = {"inflow": DeviceInflow(m, injections, c.dx**2)}
     setup = time.perf_counter() - t0
     torch.cuda.synchronize(dev)
     w0 = time.perf_counter()
-    out = run_windows(m, c.t_end, host_forcing=forcing, window=30.0, maxima=maxima, tally=tally, storage=storage)
+    out = run_windows(m, c.t_end, window=30.0, maxima=maxima, tally=tally, storage=storage, **sources)
     torch.cuda.synchronize(dev)
     wall = time.perf_counter() - w0
     b = out.balance
@@ -745,7 +858,7 @@ def main() -> None:
     dev = torch.device("cuda", local)
     if world > 1:
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=600))
-    m, c, grid, tables, maxima, tally, rate = build_workload(args.n, dev)
+    m, c, grid, tables, maxima, tally, rate = build_workload(args.n, dev, args.arith)
     b = m.backend
     cells = args.n * args.n
     tile_cells = (grid.ntiles - 1) * 1024
@@ -797,65 +910,110 @@ def main() -> None:
     faces = statistics.mean(faces_ms)
     hbm, peak_kind = peaks()
     achieved = ALG_FACES * tile_cells / (faces / 1e3) / 1e9
-    traffic = None
-    tf = ROOT / "profiles" / "faces_kernel_config3_1024.md"
-    if tf.exists():
-        for ln in tf.read_text().splitlines():
-            if ln.startswith("traffic_bytes_per_cell:"):
-                traffic = float(ln.split(":")[1]) * tile_cells  # the capture's bytes a cell, scaled to this launch
-    roofline = {"kernel": "faces_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+    traffic = FACES_DRAM_BYTES_PER_CELL * tile_cells
+    roofline = {"kernel": f"{args.arith}::faces_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": traffic,
                 "alg_bytes_per_cell": ALG_FACES, "launch_ms": faces,
                 "update_kernel_ms": statistics.mean(update_ms),
                 "step_alg_bytes_per_cell": ALG_STEP,
                 "step_frac": (cells * ran / (ms / 1e3)) * ALG_STEP / 1e9 / hbm}  # fmt: skip
 
-    # end to end through the C-ABI with host buffers: per 30 s window, the window's rain from pinned memory
+    # end to end through the C-ABI with host buffers, as the reference's run driver and monitor take a run: per 30 s
+    # window the window's rain from pinned memory, the window stepped, then what the monitor reads each window (the
+    # clock and the active list, the design line's discharge, the outfall volume, the FP64 storage); at the end the
+    # five envelope maps
+    from wadi2d_b200.maxima import Lines, faces_across
+    from wadi2d_b200.run import DeviceStorage
+    from wadi2d_b200.state import state_index
+
+    rows, cols = c.boundary_cells()
+    main = rows == rows.max()
+    line = Lines(m, [faces_across(grid, rows[main], cols[main], axis=0)])  # the main outfall's row, southward
+    jj, ii = np.nonzero(grid.mask)
+    storage = DeviceStorage(m, np.asarray(state_index(grid, jj, ii), np.int64))
+    del jj, ii
     src_native = b.native("src").cpu().pin_memory()
     win = 30.0
     h2d = d2h = 0
     torch.cuda.synchronize(dev)
     w0 = time.perf_counter()
     s0 = m.stepper.nsteps
+    series = []
     for _ in range(args.e2e_windows):
         _lib.call("w2b_set_field", b.handle, _lib.FIELD_ID["src"], src_native.data_ptr(), _lib.LAYOUT_NATIVE, 1,
                   stream.cuda_stream)  # fmt: skip
         h2d += src_native.numel() * 4
         m.run(m.stepper.t + win, maxima=maxima, tally=tally)
-        d2h += ctypes.sizeof(_lib.Clock)
+        d2h += ctypes.sizeof(_lib.Clock) + 4 * (int(b.nact) + grid.ntiles)  # the clock, the active list, idle counts
+        series.append((m.stepper.t, float(line.discharge()[0]), tally.volume(), storage()))
+        d2h += 8 * 3
+    env = [a.cpu() for a in maxima.arrays]
+    d2h += sum(a.numel() * a.element_size() for a in env)
     torch.cuda.synchronize(dev)
     e2e_s = time.perf_counter() - w0
     e2e_steps = m.stepper.nsteps - s0
     e2e = {"value": world * cells * e2e_steps / e2e_s, "unit": "cell-steps/s",
            "h2d_bytes_per_step": h2d / max(e2e_steps, 1), "d2h_bytes_per_step": d2h / max(e2e_steps, 1),
-           "windows": args.e2e_windows, "steps": e2e_steps}  # fmt: skip
+           "windows": args.e2e_windows, "steps": e2e_steps,
+           "read_back": "per window: clock, active list, design-line discharge, outfall volume, storage; at the end: "
+                        "the five envelope maps",
+           "last_window": {"t_s": series[-1][0], "line_q_m3s": series[-1][1], "outflow_m3": series[-1][2],
+                           "storage_m3": series[-1][3]} if series else None}  # fmt: skip
+    del env
 
-    cpu = None
+    wet_fraction = float((m.field("h") > 0).sum()) / cells
+    launch = b.loop_config()
+    cfl = m.num.cfl
+    memory_gb = torch.cuda.memory_allocated(dev) / 1e9
+    cpu = parity = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         threads = os.cpu_count() or 1
-        cv, done, el, ccells = cpu_sample(c, grid, rate, args.cpu_seconds, threads)
+        block = block_inputs(c, grid, rate)
+        if args.parity_steps > 0:
+            parity = block_parity(block, args.arith, args.parity_steps, threads)
+        cv, done, el, ccells = cpu_sample(block, args.cpu_seconds, threads)
         cpu = {"value": cv, "unit": "cell-steps/s", "cores": threads, "kind": "port",
                "sample": f"{CPU_BLOCK_TILES}x{CPU_BLOCK_TILES} tiles ({ccells} cells) of the workload, {done} steps "
                          f"in {el:.1f} s"}  # fmt: skip
+    sweep = None
+    if rank == 0 and world == 1 and not args.no_sweep:
+        # the other half of the metric, bounded: the critical-duration storm sweep at 128 x 128 cells, 100 candidates
+        del m, b, maxima, tally, tables
+        torch.cuda.empty_cache()
+        try:
+            r = critical_search(128, 100, 32, 4, iters=1500, arith=args.arith)
+            sweep = {"workload": f"configuration 5 reduced: {r['cells']} cells at {r['dx_m']} m, {r['candidates']} "
+                                 f"candidate storms, {r['train_runs']} training runs, top {r['top']} re-run",
+                     "runs_per_h": {"screened": r["screened"]["runs_per_h"],
+                                    "exhaustive_batched": r["exhaustive_batched"]["runs_per_h"],
+                                    "plain_one_after_another": r["plain_one_after_another"]["runs_per_h"]},
+                     "speedup_screened_vs_plain": r["speedup_screened_vs_plain"],
+                     "same_critical": r["screened"]["same_critical"],
+                     "peak_q_error": r["screened"]["peak_q_error"],
+                     "critical_in_network_top": r["screened"]["critical_in_top"],
+                     "critical_in_intensity_top": r["intensity_screen"]["critical_in_top"],
+                     "same_peaks_one_after_another": r["plain_one_after_another"]["same_peaks_as_batch"]}  # fmt: skip
+        except Exception as exc:  # the sweep is reported, never the reason the line is missing
+            sweep = {"error": f"{type(exc).__name__}: {exc}"}
     if world > 1:
         dist.barrier()
     if rank == 0:
-        wet = float((m.field("h") > 0).sum()) / cells
+        wet = wet_fraction
         line = {
             "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": world, "steps": ran,
             "warmup": args.warmup, "ms_per_step": ms / ran, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded fractal catchment, lognormal storm)",
             "config": {"workload": f"configuration 3: {args.n}x{args.n} cells at 30 m, 4x4 pixels, wet start under peak "
                                    "rain, every tile stepped, envelope every 4 steps, FP64 tally every step",
-                       "cells": cells, "tiles": grid.ntiles - 1, "wet_fraction": wet, "cfl": m.num.cfl,
-                       "l2": f"inputs larger than L2 ({torch.cuda.memory_allocated(dev) / 1e9:.1f} GB resident)",
+                       "cells": cells, "tiles": grid.ntiles - 1, "wet_fraction": wet, "cfl": cfl,
+                       "l2": f"inputs larger than L2 ({memory_gb:.1f} GB resident)",
                        "parallelism": f"replicas x{world}",
-                       "loop": "device-resident, CUDA graphs", "launch": b.loop_config(),
+                       "arith": args.arith, "loop": "device-resident, CUDA graphs", "launch": launch,
                        "tuning_steps": tune_steps},
-            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "clocks": clk,
+            "roofline": roofline, "cpu_baseline": cpu, "parity": parity, "e2e": e2e, "sweep": sweep, "clocks": clk,
             # the device loop's launches: the work list and the first step's settings, then graphs of 16 steps of
             # six kernels (faces, update, envelope, boundary, control, plan)
-            "gpu_launches": 2 + 6 * b.loop_config()["steps_per_graph"] * -(-ran // b.loop_config()["steps_per_graph"]),
+            "gpu_launches": 2 + 6 * launch["steps_per_graph"] * -(-ran // launch["steps_per_graph"]),
         }  # fmt: skip
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -60,11 +60,21 @@ typedef struct {
     int64_t ncells; /* floats per native state array: (ny + 2 gy) * px */
 } W2BLayout;
 
-/* Kernel constants: wadi2d/solver/backend.py:15-39 (NumericsRecord), plus level_fp64: the near-dry level of a cell
- * (first table interval) inverted in FP64 instead of FP32 (off reproduces the reference's arithmetic). */
+/* Kernel constants: wadi2d/solver/backend.py:15-39 (NumericsRecord), plus two switches with no counterpart in the
+ * reference:
+ *  - level_fp64: the near-dry level of a cell (first table interval) inverted in FP64 instead of FP32 (off
+ *    reproduces the reference's arithmetic);
+ *  - arith: the build of the face and update passes. W2B_ARITH_EXACT is the reference's float32 arithmetic (IEEE
+ *    division and square root, no FMA contraction, the correctly rounded cube root): the reference CPU twin's bits.
+ *    W2B_ARITH_FAST is the same step with FMA contraction and the hardware's approximate division, square root and
+ *    cube root in the face pass: fewer instructions, results within a few float32 ulp a step of the exact build's.
+ *    Other values are refused with W2B_EINVAL. Changing it through w2b_set_params restarts the launch tuner. */
+#define W2B_ARITH_EXACT 0
+#define W2B_ARITH_FAST 1
 typedef struct {
     float g, dx, e_wet, h_cfl, u_max, lead, a_min;
     int32_t second, sheet, mirror, carry, level_fp64;
+    int32_t arith;
 } W2BParams;
 
 /* Device buffers (caller-owned). Ping-pong pairs [2]: the library tracks which half is current. */
@@ -242,6 +252,31 @@ int32_t w2b_cell_size(void* handle, float* dx);
 int32_t w2b_rain_window(void* handle, const W2BRain* rain, double f0, double f1, double t0, double t1,
                         double* volume, void* stream);
 
+/* Lumped inflows of a source window on the device: the inflow part of Forcing.rate (wadi2d/forcing.py:684-694), each
+ * hydrograph's mean flow over the window shared over its cells by their level d (Injection.share,
+ * wadi2d/forcing.py:468-476), which is read in place instead of copied to the host (wadi2d/forcing.py:631-644). For
+ * each of n injections (n <= W2B_INFLOWS_MAX) with q[i] > 0 (q: host array, m3/s): the cells with d >= min_depth[i]
+ * share q[i] in proportion to d, all of it goes to the lowest cell while none does; each cell's rate
+ * (float)(q share / area) is added to src, on top of the window's rain rate where rained[cell] (the rain pass of the
+ * same window wrote src there), else on 0. volume[i] (device) = injection i's window volume (its float32 rates summed
+ * in FP64, times area and t1 - t0), and volume[n] += the window's total: the host form's numbers, in its order.
+ *   start, lowest, min_depth: host arrays (n + 1, n, n): injection i's cells are cells[start[i] .. start[i + 1]), at
+ *     most W2B_INFLOW_CELLS_MAX of them, start[0] = 0, lowest[i] the position of its lowest cell among them;
+ *   cells (NATIVE indices), rained (one byte a cell): device arrays of start[n] entries; area: the cell area, m2. */
+#define W2B_INFLOWS_MAX 64
+#define W2B_INFLOW_CELLS_MAX 4096
+typedef struct {
+    int32_t n;
+    const int32_t* start;
+    const int32_t* lowest;
+    const double* min_depth;
+    const int32_t* cells;
+    const uint8_t* rained;
+    double area;
+    double* volume;
+} W2BInflow;
+int32_t w2b_inflow_window(void* handle, const W2BInflow* inflow, const double* q, double t0, double t1, void* stream);
+
 /* Uniform sources of a batch: src at each of the n NATIVE cells = rate[run of the cell] (device array of nruns,
  * m/s). The batched form of Forcing.rate's uniform rain (wadi2d/storm/uniform.py:31-35, wadi2d/forcing.py:667-683)
  * for runs that each have a storm of their own. */
@@ -282,6 +317,10 @@ typedef struct {
     int64_t ws_threads;
 } W2BTableOut;
 
+/* The largest W2BTableIn.margin (pixels each side of a face) the builder takes with local != 0; a negative margin or
+ * a larger one is refused with W2B_EINVAL. */
+#define W2B_TABLE_MARGIN_MAX (1 << 20)
+
 /* Doubles of table-builder scratch for lines of up to nmax pixels and the given face-kernel thread count. */
 int64_t w2b_table_workspace_doubles(int32_t nmax, int64_t threads);
 
@@ -298,9 +337,12 @@ int32_t w2b_build_tables(const W2BTableIn* in, const W2BTableOut* out, void* str
  * allocating library call) and uses instead a 32 MiB array of file-scope device memory, which every GPU that loads
  * the library holds until the process exits. out->ws and out->ws_threads are ignored.
  *  - Limit: a face's line (k + 2 margin pixels) of at most 3,639 pixels; longer lines are refused with W2B_EINVAL
- *    and a message. Lines that fit the builder's shared-memory workspace (about 2,800 pixels) do not touch the array.
+ *    and a message. Lines that fit the builder's shared-memory workspace (up to 2,843 pixels) do not touch the array.
+ *    Lines of 2,844 to 3,639 pixels do, and the array holds the workspaces of only 128 to 155 threads: the face
+ *    tables are then built by a single CTA of 128 threads, correct but far slower than with a caller's workspace.
  *  - The first call on a device looks the array's address up (cudaGetSymbolAddress) with that device current;
- *    make that first call before any stream capture.
+ *    make that first call before any stream capture. The address is kept for the life of the process: it is not
+ *    valid across a cudaDeviceReset.
  *  - Every call shares the one array and it keeps the last call's contents; the kernels write every scratch slot
  *    before reading it, so nothing has to start at zero. Calls that overlap on the GPU (two streams, two threads)
  *    race on it: serialise them. */

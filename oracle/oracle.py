@@ -577,6 +577,7 @@ class Model:
         self.dt = self.num.cfl * grid.dx / self.num.wave_floor
         self.idle = np.zeros(grid.ntiles, np.int32)
         self.dts: list[float] = []
+        self.kick = None  # a momentum source on faces, applied before every step (wadi2d/solver/stepper.py:111-112)
 
     @property
     def stepper(self) -> Model:
@@ -642,6 +643,10 @@ class Model:
         self.keep_active[self.boundary_tiles] = True
         self.rebuild_active(retain=True)
 
+    def set_momentum(self, kick) -> None:
+        """A momentum source on faces for the steps until the next call (wadi2d/solver/model.py:128-132)."""
+        self.kick = kick
+
     def cell_state_index(self, j: int, i: int) -> int:
         return int(state_index(self.grid, j, i))
 
@@ -687,6 +692,8 @@ class Model:
             self.refresh_due = False
             activate = self.nsteps % num.active_every == 0
             dt = min(self.dt, t_end - self.t, num.dt_max)
+            if self.kick is not None:
+                self.kick.apply(b, dt)
             b.step(dt, refresh, activate)
             self.dts.append(dt)
             self.t += dt

@@ -2,7 +2,7 @@
 
 Run in a container that holds the reference source tree (read-only is fine):
 
-    WADI2D_REFERENCE=/root/reference NUMBA_CACHE_DIR=/tmp/numba_cache PYTHONDONTWRITEBYTECODE=1 \
+    WADI2D_REFERENCE=<the reference source tree> NUMBA_CACHE_DIR=/tmp/numba_cache PYTHONDONTWRITEBYTECODE=1 \
         python tests/golden/make_golden.py
 
 It imports ``wadi2d`` from that tree and drives ``Model(..., "cpu")`` (the Numba twin of the reference's GPU
@@ -26,7 +26,9 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 sys.path.insert(0, str(HERE.parents[1]))
 sys.path.insert(0, str(HERE))
-sys.path.insert(0, os.environ.get("WADI2D_REFERENCE", "/root/reference"))
+if not os.environ.get("WADI2D_REFERENCE"):
+    sys.exit("set WADI2D_REFERENCE to the reference source tree")
+sys.path.insert(0, os.environ["WADI2D_REFERENCE"])
 
 from wadi2d.config.schema import Numerics, Tables  # noqa: E402
 from wadi2d.engine.maxima import Maxima, Tally  # noqa: E402

@@ -1,7 +1,7 @@
 """Golden vectors of the reference's loss, storm and ARF arithmetic (the parts of its forcing that import without
 its GIS dependencies). Run where the reference tree is importable:
 
-    WADI2D_REFERENCE=/root/reference PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden_forcing.py
+    WADI2D_REFERENCE=<the reference source tree> PYTHONDONTWRITEBYTECODE=1 python tests/golden/make_golden_forcing.py
 
 It writes tests/golden/forcing.npz: SCS cumulative excess over curve numbers x depths (with and without a given
 initial abstraction), ARF table factors over areas (both ends' rules), uniform-storm cumulative depths, and the
@@ -18,7 +18,9 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-sys.path.insert(0, os.environ.get("WADI2D_REFERENCE", "/root/reference"))
+if not os.environ.get("WADI2D_REFERENCE"):
+    sys.exit("set WADI2D_REFERENCE to the reference source tree")
+sys.path.insert(0, os.environ["WADI2D_REFERENCE"])
 
 
 class _Stub:

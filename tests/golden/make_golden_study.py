@@ -3,7 +3,7 @@ inputs.
 
 Run in a container that holds the reference source tree (read-only is fine):
 
-    WADI2D_REFERENCE=/root/reference python tests/golden/make_golden_study.py
+    WADI2D_REFERENCE=<the reference source tree> python tests/golden/make_golden_study.py
 
 The reference's study module (wadi2d/arf.py) imports its I/O stack (rasterio, h5py and the products) at the top, which
 this image does not have, so the script reads the module's source, takes the definitions of its pure numpy helpers
@@ -24,7 +24,9 @@ from pathlib import Path
 import numpy as np
 
 HERE = Path(__file__).resolve().parent
-REF = Path(os.environ.get("WADI2D_REFERENCE", "/root/reference"))
+if not os.environ.get("WADI2D_REFERENCE"):
+    sys.exit("set WADI2D_REFERENCE to the reference source tree")
+REF = Path(os.environ["WADI2D_REFERENCE"])
 WANTED = ("bracket_areas", "storm_areas", "run_name", "interpolate_peak", "_row", "interpolated_row",
           "log_area_weights", "composite_map")  # fmt: skip
 

@@ -1,6 +1,7 @@
 """The adapter of tests/golden/cases.py onto this package's CUDA path. Tables come from ``table_source``: the oracle
 (test infrastructure, pinned to the reference) by default, so a step comparison sees the reference's own tables;
-``"gpu"`` builds them with the package's GPU builder instead."""
+``"gpu"`` builds them with the package's GPU builder instead. ``arith`` picks the step's build: ``"exact"`` (the
+reference's float32 bits) or ``"fast"``."""
 
 from __future__ import annotations
 
@@ -14,10 +15,11 @@ from wadi2d_b200.model import Model
 
 
 class B200Api:
-    def __init__(self, table_source: str = "oracle", device_loop: bool = False) -> None:
+    def __init__(self, table_source: str = "oracle", device_loop: bool = False, arith: str = "exact") -> None:
         self.dts: list[float] = []
         self.table_source = table_source
         self.device_loop = device_loop
+        self.arith = arith
         self.models: list[Model] = []
 
     def grid(self, mask, x0, y0, dx):
@@ -32,7 +34,7 @@ class B200Api:
         return T.GridTables.from_dict(grid, d)
 
     def model(self, grid, tables, numerics):
-        m = Model(tables, Numerics(**numerics))
+        m = Model(tables, Numerics(**numerics, arithmetic=self.arith))
         step = m.backend.step
 
         def logged(dt, want_wave, want_wet):

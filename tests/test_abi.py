@@ -76,3 +76,18 @@ def test_every_entry_point_refuses_null_arguments_without_a_gpu():
         assert getattr(L, name)(*zeros) == _lib.EINVAL, name
     assert L.w2b_version() == 2
     assert L.w2b_run_table_bytes(0) == 0
+
+
+def test_table_build_refuses_a_bad_margin_without_a_gpu():
+    """With the local radius on, a negative margin or one beyond W2B_TABLE_MARGIN_MAX is refused before any device
+    work, by both table-build entry points."""
+    from wadi2d_b200.tablebuild import TableIn, TableOut
+
+    L = _lib.lib()
+    fake = 256  # never dereferenced: the arguments are checked first
+    for margin in (-1, (1 << 20) + 1, -(1 << 30)):
+        tin = TableIn(fake, 64, 64, 0, 0, None, fake, None, None, None, None, None, None, None, None, fake, fake, 2, 32,
+                      32, 2, 16, 1, margin, 1.0, 8.0, 16.0, 9.0, 0.05)  # fmt: skip
+        out = TableOut(*([None] * 22), fake, 128)
+        assert L.w2b_build_tables(ctypes.byref(tin), ctypes.byref(out), None) == _lib.EINVAL, margin
+        assert L.w2b_build_tables_noalloc(ctypes.byref(tin), ctypes.byref(out), None) == _lib.EINVAL, margin

@@ -29,7 +29,7 @@ def test_cpu_sample_steps_the_oracle_on_the_block():
     c = types.SimpleNamespace(dx=30.0, k=k, manning=0.035)
     c.block_z = bed[j0 * k : (j0 + side) * k + 2, i0 * k : (i0 + side) * k + 2]
     rate = np.full(grid.shape, 40.0 / 3.6e6)
-    value, done, seconds, cells = bench.cpu_sample(c, grid, rate, 0.0, 2, steps=2, warmup=1)
+    value, done, seconds, cells = bench.cpu_sample(bench.block_inputs(c, grid, rate), 0.0, 2, steps=2, warmup=1)
     assert cells == side * side == 1_048_576
     assert done == 2 and seconds > 0.0
     assert value == cells * done / seconds

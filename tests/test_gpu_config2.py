@@ -1,6 +1,7 @@
-"""Configuration 2 at a reduced size on the B200: crest faces from seeded breaklines, three lumped inflows shared over
-their cells by depth through the window driver (wadi2d/forcing.py:667-695, depths read from the device as
-wadi2d/forcing.py:631-644 does), a reservoir started at its level (hbar_at_level), Manning patches and a free outfall.
+"""Configuration 2 at reduced sizes (96 x 96 and 256 x 256 cells) on the B200: crest faces from seeded breaklines,
+three lumped inflows shared over their cells by depth through the window driver (wadi2d/forcing.py:667-695, depths
+read from the device as wadi2d/forcing.py:631-644 does), a reservoir started at its level (hbar_at_level), Manning
+patches and a free outfall.
 The step on the oracle's tables against the oracle's run field by field within the step's accuracy tolerances, the
 GPU-built tables against the oracle's within one ulp, and the FP64 books closing."""
 
@@ -21,13 +22,13 @@ from wadi2d_b200.state import state_index
 from wadi2d_b200.tables import ArrayBed, GridTables, build_tables, hbar_at_level
 
 pytestmark = pytest.mark.gpu
-N, K, T_END, WINDOW = 96, 4, 1800.0, 30.0
+K, T_END, WINDOW = 4, 1800.0, 30.0
 TABLE_FIELDS = ("hc", "dtab", "flx", "frx", "glx", "grx", "efx", "cwx", "ftabx", "fly", "fry", "gly", "gry", "efy",
                 "cwy", "ftaby", "zcx", "zcy")  # fmt: skip
 
 
-def _inputs():
-    c = workloads.crest_valley(n=N, k=K, breaklines=10, t_end=T_END)
+def _inputs(N: int = 96):
+    c = workloads.crest_valley(n=N, k=K, breaklines=10 if N <= 96 else 20, t_end=T_END)
     mask = np.ones((N, N), bool)
     og = O.Grid.from_mask(mask, 0.0, 0.0, c.dx)
     g = TileGrid.from_mask(mask, 0.0, 0.0, c.dx)
@@ -91,8 +92,9 @@ def _drive(model, forcing, tally, device: bool):
     return inflow
 
 
-def test_configuration2_small_matches_the_oracle_and_balances():
-    c, og, g, tab = _inputs()
+@pytest.mark.parametrize("N", [96, 256])
+def test_configuration2_small_matches_the_oracle_and_balances(N):
+    c, og, g, tab = _inputs(N)
     O.threads(0)
     om = O.Model(og, tab, O.Numerics())
     of, ot, _, _ = _setup(c, g, om, tab, O.Tally, O.Boundary)

@@ -73,15 +73,27 @@ def exact(variant: str, s: np.ndarray) -> tuple[np.ndarray, np.ndarray]:
     return depth, bed
 
 
-def steady(variant: str, t_end: float = 2500.0):
-    """The run of tests/solver/test_steady.py:17-64 on the oracle: (depth, unit discharge) on the channel's cells."""
+def steady(variant: str, t_end: float = 2500.0, on: str = "oracle", arith: str = "exact"):
+    """The run of tests/solver/test_steady.py:17-64 on the oracle, or (``on="b200"``) on this package's CUDA path with
+    the oracle's tables and the ``arith`` build: (depth, unit discharge) on the channel's cells, and the model."""
     g = O.Grid.from_mask(np.ones((NY, NX), bool), 0.0, 0.0, DX)
     ny, nx = g.shape
     x = (np.arange(nx) - PAD + 0.5) * DX  # cell centres of the padded grid, one pixel a cell
     h_cells, bed_cells = exact(variant, x)
     z = np.broadcast_to(bed_cells, (ny, nx)).copy()
     tables = O.build_tables(g, z, DX, N)
-    m = O.Model(g, tables, O.Numerics(dt_every=1, e_wet=1e-5))
+    Boundary = O.Boundary
+    if on == "oracle":
+        m = O.Model(g, tables, O.Numerics(dt_every=1, e_wet=1e-5))
+    else:
+        from wadi2d_b200.backend import BoundaryCells as Boundary
+        from wadi2d_b200.config import Numerics
+        from wadi2d_b200.grid import TileGrid
+        from wadi2d_b200.model import Model
+        from wadi2d_b200.tables import GridTables
+
+        tg = TileGrid(g.x0, g.y0, g.dx, g.mask)
+        m = Model(GridTables.from_dict(tg, tables), Numerics(dt_every=1, e_wet=1e-5, arithmetic=arith))
     h0 = np.broadcast_to(h_cells, (ny, nx))
     m.set_depth(h0)
     m.set_velocity(Q / h0, np.zeros((ny, nx)))
@@ -95,9 +107,9 @@ def steady(variant: str, t_end: float = 2500.0):
     held = [] if sub_in else inlet
     d_out = h_out if sub_out else 0.0
     depths = [h_in] * len(held) + [d_out] * NY
-    m.set_boundary(O.Boundary(np.array(held + last, np.int32), np.array(held + before_last, np.int32),
-                              np.array([0] * len(held) + [0 if sub_out else 2] * NY, np.int32),
-                              np.array(depths, np.float32), np.array(depths, np.float32)))  # fmt: skip
+    m.set_boundary(Boundary(np.array(held + last, np.int32), np.array(held + before_last, np.int32),
+                            np.array([0] * len(held) + [0 if sub_out else 2] * NY, np.int32),
+                            np.array(depths, np.float32), np.array(depths, np.float32)))  # fmt: skip
     if sub_in:
         rate = np.zeros((ny, nx))
         rate[PAD : PAD + NY, PAD] = Q / DX
@@ -117,12 +129,15 @@ def steady(variant: str, t_end: float = 2500.0):
     sl = (slice(PAD, PAD + NY), slice(PAD, PAD + NX))
     qxf = m.field("qx")
     qx = 0.5 * (qxf + np.roll(qxf, -1, axis=1))[sl] / DX
-    return m.field("h")[sl].astype(np.float64), qx.astype(np.float64)
+    return m.field("h")[sl].astype(np.float64), qx.astype(np.float64), m
 
 
-@pytest.mark.parametrize(("variant", "limit"), [("subcritical", 0.015), ("supercritical", 0.012), ("jump", 0.05)])
+LIMITS = [("subcritical", 0.015), ("supercritical", 0.012), ("jump", 0.05)]
+
+
+@pytest.mark.parametrize(("variant", "limit"), LIMITS)
 def test_macdonald(variant, limit):
-    h, qx = steady(variant)
+    h, qx, _ = steady(variant)
     want, _ = exact(variant, (np.arange(NX) + 0.5) * DX)
     err = float(np.sqrt(np.mean((h[1, 2:-2] - want[2:-2]) ** 2)))
     assert err < limit, f"{variant}: depth RMSE {err:.4f} m"

@@ -3,8 +3,11 @@
 Such a caller (a host program whose device memory belongs to a pool or caching allocator it does not control, or an
 FFI binding with no allocator of its own) passes inputs and outputs but no scratch; the entry point uses the
 library's own fixed 32 MiB device array instead. Here it is called twice in a row through the C-ABI, and each result
-must equal, bit for bit, the tables of the entry point that takes the caller's scratch. This file is collected last,
-so a run that stops at its first failure has already run every other test; it also passes alone in a fresh process.
+must equal, bit for bit, the tables of the entry point that takes the caller's scratch. Two face-line lengths:
+configuration 1's (149 pixels), whose local-radius workspace fits in shared memory, and one of 3,005 pixels (a
+margin of 1,500 pixels), beyond the 2,843 pixels shared memory holds, so the face-table kernel works in the static
+array itself. This file is collected last, so a run that stops at its first failure has already run every other
+test; it also passes alone in a fresh process.
 """
 
 from __future__ import annotations
@@ -57,7 +60,12 @@ def _marshal(torch, dev, grid, z, pixel, manning, local, margin):
     return tin, outputs, keep, TableOut
 
 
-def test_noalloc_table_build_equals_the_scratch_build_twice_in_a_row():
+SHARED_LINE_MAX = 204800 // (9 * 8) - 1  # 2,843: the longest line whose workspace fits a CTA's 200 KiB
+ARRAY_LINE_MAX = (32 << 20) // (128 * 9 * 8) - 1  # 3,639: the longest line the 32 MiB array holds for 128 threads
+
+
+@pytest.mark.parametrize("n, margin", [(64, None), (30, 1500)], ids=["shared_memory_lines", "static_array_lines"])
+def test_noalloc_table_build_equals_the_scratch_build_twice_in_a_row(n, margin):
     import torch
 
     from wadi2d_b200 import _lib
@@ -66,9 +74,13 @@ def test_noalloc_table_build_equals_the_scratch_build_twice_in_a_row():
     lib = _lib.lib()
     dev = torch.device("cuda")
     stream = torch.cuda.current_stream().cuda_stream
-    grid, (z, pixel, manning, local, _, _), _ = cases.c1_small_inputs(OracleApi())
+    grid, (z, pixel, manning, local, _, _), _ = cases.c1_small_inputs(OracleApi(), n=n)
     k = round(grid.dx / pixel)
-    margin = int(min(np.ceil(9.0 * 16.0 / pixel), max(z.shape)))
+    if margin is None:
+        margin = int(min(np.ceil(9.0 * 16.0 / pixel), max(z.shape)))
+        assert k + 2 * margin <= SHARED_LINE_MAX
+    else:
+        assert SHARED_LINE_MAX < k + 2 * margin <= ARRAY_LINE_MAX  # the face kernel's workspace is the array
     tin, outputs, keep, TableOut = _marshal(torch, dev, grid, z, pixel, manning, local, margin)
     names = TILE_FIELDS + ("zmin", "rel", "zfx", "zfy")
 
@@ -80,7 +92,7 @@ def test_noalloc_table_build_equals_the_scratch_build_twice_in_a_row():
     lib.w2b_build_tables_noalloc.restype = ctypes.c_int32
 
     # the entry point that takes the caller's scratch
-    threads = 148 * 8 * 128
+    threads = 148 * 8 * 128 if k + 2 * margin <= SHARED_LINE_MAX else 1024
     ws = torch.empty(9 * (k + 2 * margin + 1) * threads, dtype=torch.float64, device=dev)
     ref = outputs()
     assert lib.w2b_build_tables(ctypes.byref(tin), ctypes.byref(out_struct(ref, ws, threads)), stream) == 0

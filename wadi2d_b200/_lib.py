@@ -11,6 +11,8 @@ c_i32, c_i64, c_f32, c_f64, c_vp = ctypes.c_int32, ctypes.c_int64, ctypes.c_floa
 
 OK, EINVAL, ECUDA, ENONFINITE, EDTMIN, ETIMEOUT = 0, -1, -2, -3, -4, -5
 LAYOUT_REF_TILE, LAYOUT_NATIVE = 0, 1
+ARITH_EXACT, ARITH_FAST = 0, 1
+ARITH = {"exact": ARITH_EXACT, "fast": ARITH_FAST}
 FIELDS = ("h", "d", "u", "v", "mx", "my", "qx", "qy", "u1", "v1", "mx1", "my1", "qx1", "qy1", "src", "res", "om",
           "zcx", "zcy")  # fmt: skip
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
@@ -37,7 +39,7 @@ class Layout(ctypes.Structure):
 
 class Params(ctypes.Structure):
     _fields_ = [(n, c_f32) for n in ("g", "dx", "e_wet", "h_cfl", "u_max", "lead", "a_min")] + [
-        (n, c_i32) for n in ("second", "sheet", "mirror", "carry", "level_fp64")
+        (n, c_i32) for n in ("second", "sheet", "mirror", "carry", "level_fp64", "arith")
     ]
 
 
@@ -65,6 +67,12 @@ class Rain(ctypes.Structure):
 
 
 PARTIALS = 296
+INFLOWS_MAX, INFLOW_CELLS_MAX = 64, 4096
+
+
+class Inflow(ctypes.Structure):
+    _fields_ = [("n", c_i32), ("start", c_vp), ("lowest", c_vp), ("min_depth", c_vp), ("cells", c_vp),
+                ("rained", c_vp), ("area", c_f64), ("volume", c_vp)]  # fmt: skip
 
 
 class Clock(ctypes.Structure):
@@ -117,6 +125,7 @@ _SIGNATURES = {
     "w2b_advance_runs": [c_vp, ctypes.POINTER(Stepper), c_vp, c_i64, c_vp, c_vp],
     "w2b_cell_size": [c_vp, ctypes.POINTER(c_f32)],
     "w2b_rain_window": [c_vp, c_vp, c_f64, c_f64, c_f64, c_f64, c_vp, c_vp],
+    "w2b_inflow_window": [c_vp, c_vp, c_vp, c_f64, c_f64, c_vp],
     "w2b_storage": [c_vp, c_i64, c_vp, c_vp, c_vp, c_vp],
 }
 

@@ -38,6 +38,7 @@ class NumericsRecord:
     mirror: bool
     carry: bool = True
     level_fp64: bool = False
+    arith: str = "exact"
 
     @classmethod
     def from_config(cls, num: Numerics, dx: float) -> NumericsRecord:
@@ -45,6 +46,7 @@ class NumericsRecord:
         return cls(
             G, dx, num.e_wet, num.h_cfl, num.u_max, lead, num.plan_min, num.limiter != "none", num.sheet_flow,
             num.mirror_dry_faces, num.face_depth_carry, bool(getattr(num, "level_fp64", False)),
+            str(getattr(num, "arithmetic", "exact")),
         )  # fmt: skip
 
 
@@ -246,6 +248,7 @@ class B200Backend:
         return _lib.Params(
             num.g, num.dx, num.e_wet, num.h_cfl, num.u_max, num.lead, num.a_min, int(num.second), int(num.sheet),
             int(num.mirror), int(num.carry), int(getattr(num, "level_fp64", False)),
+            _lib.ARITH[getattr(num, "arith", "exact")],
         )  # fmt: skip
 
     def _stream(self) -> int:

@@ -40,6 +40,10 @@ class Numerics:
     lts_levels: int = 3
     level_fp64: bool = False
     """Invert the near-dry bottom interval of each cell table in FP64 (not in the reference; off reproduces it)."""
+    arithmetic: str = "exact"
+    """The build of the step's face and update passes (not in the reference): "exact" is the reference's float32
+    arithmetic, its CPU twin's bits; "fast" adds FMA contraction and the hardware's approximate division, square root
+    and cube root in the face pass."""
 
     def validate(self) -> Numerics:
         """The reference's bounds (wadi2d/config/schema.py:457-519); cfl up to 0.7."""
@@ -49,7 +53,7 @@ class Numerics:
             (1.0 <= self.u_max <= 100.0, "u_max"), (1e-3 <= self.dt_max <= 600.0, "dt_max"),
             (1e-6 <= self.dt_min <= 1.0, "dt_min"), (1 <= self.dt_every <= 64, "dt_every"),
             (0.1 <= self.wave_floor <= 30.0, "wave_floor"), (1e-4 <= self.plan_min <= 1.0, "plan_min"),
-            (1 <= self.active_every <= 32, "active_every"),
+            (1 <= self.active_every <= 32, "active_every"), (self.arithmetic in ("exact", "fast"), "arithmetic"),
         ]  # fmt: skip
         bad = [n for ok, n in checks if not ok]
         if bad:

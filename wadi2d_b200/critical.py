@@ -217,6 +217,7 @@ class Catchment5:
     tally: tuple
     rained: np.ndarray
     lines: list
+    relief: float = 0.0
 
 
 def prepare(n: int = 256, dx: float = 10.0, k: int = 4, seed: int = 17, relief: float | None = None,
@@ -231,8 +232,8 @@ def prepare(n: int = 256, dx: float = 10.0, k: int = 4, seed: int = 17, relief: 
     from wadi2d_b200.state import state_index
     from wadi2d_b200.tables import ArrayBed, build_tables
 
-    c = workloads.catchment(n=n, dx=dx, k=k, seed=seed, relief=relief if relief is not None else 0.03 * n * dx,
-                            device=device)  # fmt: skip
+    relief = relief if relief is not None else 0.03 * n * dx
+    c = workloads.catchment(n=n, dx=dx, k=k, seed=seed, relief=relief, device=device)
     grid = TileGrid.from_mask(np.ones((n, n), bool), 0.0, 0.0, dx)
     tables = build_tables(grid, ArrayBed(c.z, dx / k), Tables(), c.manning, device=device)
     del c.z
@@ -247,7 +248,7 @@ def prepare(n: int = 256, dx: float = 10.0, k: int = 4, seed: int = 17, relief: 
     (xf, xs), (yf, ys) = F.open_faces(grid, inner, taken)
     zmin = np.asarray(tables.zmin)
     lines = design_lines(grid, zmin)
-    return Catchment5(grid, tables, bc, (xf, xs, yf, ys), state_index(grid, jj, ii).astype(np.int64), lines)
+    return Catchment5(grid, tables, bc, (xf, xs, yf, ys), state_index(grid, jj, ii).astype(np.int64), lines, relief)
 
 
 def solve(cat: Catchment5, storms: list[MixedStorm], recession_h: float = 1.0, batch: int = 256, num=None) -> dict:

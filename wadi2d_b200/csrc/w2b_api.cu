@@ -14,15 +14,42 @@
 #include "w2b_tma.cuh"
 
 namespace w2b {
-cudaError_t faces_setup();
-void launch_probe(const StepArgs& A, int t, float dt, float* out, cudaStream_t s);
+// The face and update passes of w2b_step.cu, built twice: exact (the reference's float32 bits) and fast.
+#define W2B_PASSES_DECL                                                             \
+    cudaError_t faces_setup();                                                      \
+    void launch_probe(const StepArgs& A, int t, float dt, float* out, cudaStream_t s); \
+    int faces_occupancy();                                                          \
+    void launch_faces(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s); \
+    cudaError_t update_setup();                                                     \
+    int update_occupancy();                                                         \
+    void launch_update(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s);
+namespace exact {
+W2B_PASSES_DECL
+}
+namespace fast {
+W2B_PASSES_DECL
+}
+#undef W2B_PASSES_DECL
+
+struct Passes {
+    cudaError_t (*faces_setup)();
+    void (*launch_probe)(const StepArgs&, int, float, float*, cudaStream_t);
+    int (*faces_occupancy)();
+    void (*launch_faces)(const TMaps&, const StepArgs&, int, cudaStream_t);
+    cudaError_t (*update_setup)();
+    int (*update_occupancy)();
+    void (*launch_update)(const TMaps&, const StepArgs&, int, cudaStream_t);
+};
+static const Passes EXACT_PASSES = {exact::faces_setup,  exact::launch_probe,     exact::faces_occupancy,
+                                    exact::launch_faces, exact::update_setup,     exact::update_occupancy,
+                                    exact::launch_update};
+static const Passes FAST_PASSES = {fast::faces_setup,  fast::launch_probe,     fast::faces_occupancy,
+                                   fast::launch_faces, fast::update_setup,     fast::update_occupancy,
+                                   fast::launch_update};
+static const Passes& passes(const W2BParams& P) { return P.arith == W2B_ARITH_FAST ? FAST_PASSES : EXACT_PASSES; }
+
 void launch_cbrt_check(uint32_t first, uint32_t count, unsigned long long* out, cudaStream_t s);
 void launch_wait_check(uint32_t polls, long long* out, cudaStream_t s);
-int faces_occupancy();
-void launch_faces(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s);
-cudaError_t update_setup();
-int update_occupancy();
-void launch_update(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s);
 __global__ void boundary_kernel(StepArgs A, int control);
 __global__ void envelope_kernel(StepArgs A);
 __global__ void control_kernel(StepArgs A);
@@ -308,6 +335,23 @@ static int boundary_grid(const Handle& H, int control) {
     return (int)(g < 1 ? 1 : (g > cap ? cap : g));
 }
 
+// The shared-memory limits of both builds' passes, and the resident CTAs a SM of the handle's build (W2BParams.arith),
+// which set the launch grids and the tuner's candidates.
+static int set_passes(Handle& H) {
+    for (const Passes* X : {&EXACT_PASSES, &FAST_PASSES}) {
+        if (X->update_setup() != cudaSuccess || X->faces_setup() != cudaSuccess)
+            return cuda_status(cudaGetLastError(), "pass setup");
+    }
+    const Passes& X = passes(H.P);
+    const int occ = X.update_occupancy(), focc = X.faces_occupancy();
+    H.update_occ = occ > 0 ? occ : 1;
+    H.faces_occ = focc > 0 ? focc : 1;
+    H.step_blocks = H.sms * H.update_occ;
+    H.faces_blocks = H.sms * H.faces_occ;
+    init_loop(H);
+    return W2B_OK;
+}
+
 // One step of the device loop under launch configuration C: every running run advances by one of its own steps.
 static int launch_loop_step(Handle& H, const LoopConfig& C, cudaStream_t s) {
     StepArgs A = make_args(H);
@@ -316,8 +360,9 @@ static int launch_loop_step(Handle& H, const LoopConfig& C, cudaStream_t s) {
     const int grid = blocks_for(H, H.g.ntiles - 1);
     const int tiles = H.g.ntiles - 1 > 0 ? H.g.ntiles - 1 : 1;
     const int fgrid = H.sms * C.faces_per_sm, ugrid = H.sms * C.update_per_sm;
-    launch_faces(H.tmaps, A, tiles < fgrid ? tiles : fgrid, s);
-    launch_update(H.tmaps, A, tiles < ugrid ? tiles : ugrid, s);
+    const Passes& X = passes(H.P);
+    X.launch_faces(H.tmaps, A, tiles < fgrid ? tiles : fgrid, s);
+    X.launch_update(H.tmaps, A, tiles < ugrid ? tiles : ugrid, s);
     envelope_kernel<<<H.sms * 2, TILE2, 0, s>>>(A);
     boundary_kernel<<<boundary_grid(H, 1), 256, 0, s>>>(A, 1);
     control_kernel<<<1, 1024, 0, s>>>(A);  // clocks, rebuild and work list, the next step's settings
@@ -380,6 +425,7 @@ int32_t w2b_ref_to_native(const W2BGridDesc* grid, const int32_t* tiles_host, in
 int32_t w2b_create(const W2BGridDesc* grid, const W2BParams* params, const W2BBuffers* buffers, void** handle) {
     if (!grid || !params || !buffers || !handle) return W2B_EINVAL;
     if (grid->rows < 4 || grid->rows > 64 || grid->nruns < 1) return W2B_EINVAL;
+    if (params->arith != W2B_ARITH_EXACT && params->arith != W2B_ARITH_FAST) return W2B_EINVAL;
     if (!buffers->runs || ((uintptr_t)buffers->runs & 255) || !buffers->tile_run || !buffers->work) return W2B_EINVAL;
     {
         // arrays the passes stage with bulk copies: 16-byte aligned
@@ -403,21 +449,10 @@ int32_t w2b_create(const W2BGridDesc* grid, const W2BParams* params, const W2BBu
     int dev = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&H->sms, cudaDevAttrMultiProcessorCount, dev);
-    if (update_setup() != cudaSuccess) {
+    if (set_passes(*H) != W2B_OK) {
         delete H;
-        return cuda_status(cudaGetLastError(), "w2b_create update_setup");
+        return W2B_ECUDA;
     }
-    const int occ = update_occupancy();
-    H->step_blocks = H->sms * (occ > 0 ? occ : 1);
-    if (faces_setup() != cudaSuccess) {
-        delete H;
-        return cuda_status(cudaGetLastError(), "w2b_create faces_setup");
-    }
-    const int focc = faces_occupancy();
-    H->faces_blocks = H->sms * (focc > 0 ? focc : 1);
-    H->faces_occ = focc > 0 ? focc : 1;
-    H->update_occ = occ > 0 ? occ : 1;
-    init_loop(*H);
     if (build_tmaps(*H) != W2B_OK) {
         delete H;
         return W2B_ECUDA;
@@ -475,9 +510,16 @@ int32_t w2b_pack_tables(const W2BGridDesc* grid, const float* dtab, const float*
 
 int32_t w2b_set_params(void* handle, const W2BParams* params) {
     if (!handle || !params) return W2B_EINVAL;
+    if (params->arith != W2B_ARITH_EXACT && params->arith != W2B_ARITH_FAST) return W2B_EINVAL;
     Handle* H = static_cast<Handle*>(handle);
+    const int arith = H->P.arith;
     H->P = *params;
     H->version++;
+    if (params->arith != arith) {  // the other build's passes: their occupancy, and the tuner starts again
+        drop_graphs(*H);
+        const int st = set_passes(*H);
+        if (st != W2B_OK) return st;
+    }
     if (H->nruns == 1) CK(cudaMemcpy(H->R.dx, &H->P.dx, sizeof(float), cudaMemcpyHostToDevice));
     return W2B_OK;
 }
@@ -554,8 +596,8 @@ int32_t w2b_step(void* handle, float dt, int32_t want_wave, int32_t want_wet, vo
         return W2B_OK;
     }
     const int grid = blocks_for(*H, H->nact);
-    launch_faces(H->tmaps, A, faces_grid(*H, H->nact), s);
-    launch_update(H->tmaps, A, grid, s);
+    passes(H->P).launch_faces(H->tmaps, A, faces_grid(*H, H->nact), s);
+    passes(H->P).launch_update(H->tmaps, A, grid, s);
     if (H->nb) boundary_kernel<<<boundary_grid(*H, 0), 256, 0, s>>>(A, 0);
     endstep_kernel<<<1, 1, 0, s>>>(A);
     CKL("w2b_step");
@@ -575,9 +617,9 @@ int32_t w2b_step_timed(void* handle, float dt, int32_t want_wave, int32_t want_w
     setstep_kernel<<<1, 1, 0, s>>>(A, dt, want_wave, want_wet, H->nact);
     const int grid = blocks_for(*H, H->nact);
     CK(cudaEventRecord(ev[0], s));
-    launch_faces(H->tmaps, A, faces_grid(*H, H->nact), s);
+    passes(H->P).launch_faces(H->tmaps, A, faces_grid(*H, H->nact), s);
     CK(cudaEventRecord(ev[1], s));
-    launch_update(H->tmaps, A, grid, s);
+    passes(H->P).launch_update(H->tmaps, A, grid, s);
     CK(cudaEventRecord(ev[2], s));
     if (H->nb) boundary_kernel<<<boundary_grid(*H, 0), 256, 0, s>>>(A, 0);
     endstep_kernel<<<1, 1, 0, s>>>(A);
@@ -936,7 +978,7 @@ int32_t w2b_face_waves(void* handle, int32_t tile, float dt, float* out, void* s
     if (!handle || !out || !(dt > 0.0f)) return W2B_EINVAL;
     Handle* H = static_cast<Handle*>(handle);
     if (tile < 1 || tile >= H->g.ntiles) return W2B_EINVAL;
-    launch_probe(make_args(*H), tile, dt, out, (cudaStream_t)stream);
+    passes(H->P).launch_probe(make_args(*H), tile, dt, out, (cudaStream_t)stream);
     CKL("w2b_face_waves");
     return W2B_OK;
 }

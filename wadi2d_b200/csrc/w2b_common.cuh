@@ -236,6 +236,39 @@ __device__ __forceinline__ float cbrt32(float x) {
     if (fabsf(z) <= x * 0x1p-42f) return cbrt32_exact(x);
     return (z > 0.0f) == (d >= 0.0f) ? nb : y;
 }
+// The face pass's division, square root and cube root. The library's default build is the reference's arithmetic:
+// IEEE division and square root (it is compiled with -prec-div=true -prec-sqrt=true -fmad=false) and the correctly
+// rounded cube root, so these are a / b, sqrtf and cbrt32. The step's second build (W2B_FAST, compiled with FMA
+// contraction; selected per handle by W2BParams.arith) uses the hardware's approximations where the face pass spends
+// its instructions:
+//  - division as __fdividef (rcp.approx times the numerator, within 2 ulp while the denominator's magnitude lies in
+//    [2^-126, 2^126]: every denominator of the face pass is a depth, area, width, cell size or clamp of them, bounded
+//    below by 1e-30 or by e_wet);
+//  - sqrt.approx.f32 (within about 1 ulp; no denormal flushing);
+//  - the cube root of x >= 0 from the hardware log2 and exp2 estimates (within about 2^-18 relative) refined by one
+//    Newton step, y - (y^3 - x) / (3 y^2), which squares that error away: within a few ulp. x = 0, and x so small that
+//    the estimate is 0, give 0.
+__device__ __forceinline__ float sqrt_approx(float x) {
+    float y;
+    asm("sqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float cbrt_fast(float x) {
+    const float y0 = ex2_approx(lg2_approx(x) * 0.333333343f);
+    const float p = y0 * y0;
+    const float y = fmaf(-fmaf(p, y0, -x), rcp_approx(3.0f * p), y0);
+    return y0 > 0.0f ? y : y0;
+}
+#ifdef W2B_FAST
+__device__ __forceinline__ float qdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ float qsqrt(float x) { return sqrt_approx(x); }
+__device__ __forceinline__ float qcbrt(float x) { return cbrt_fast(x); }
+#else
+__device__ __forceinline__ float qdiv(float a, float b) { return a / b; }
+__device__ __forceinline__ float qsqrt(float x) { return sqrtf(x); }
+__device__ __forceinline__ float qcbrt(float x) { return cbrt32(x); }
+#endif
+
 // Python max/min on two ordered floats (the first argument wins a tie).
 __device__ __forceinline__ float fmax32(float a, float b) { return a >= b ? a : b; }
 __device__ __forceinline__ float fmin32(float a, float b) { return a <= b ? a : b; }
@@ -295,7 +328,8 @@ __device__ __forceinline__ float cell_plan(float hb, float hc, const float2* __r
     return hc * (float)(2 * r + 1) / (m * m) / fmax32(p.y - p.x, 1e-12f);
 }
 
-// Area, conveyance^(3/5) and wet width at depth e over the face invert, wadi2d/solver/gpu/kernels/common.cuh:64-91.
+// Area, conveyance^(3/5) and wet width at depth e over the face invert, wadi2d/solver/gpu/kernels/common.cuh:64-91
+// (with the face pass's division and square root).
 // quad(r) = (A_r, T_r, A_r+1, T_r+1).
 __device__ __forceinline__ void face_lookup(float e, float top, const float4* __restrict__ quads, int rows, float& A,
                                             float& T, float& W) {
@@ -305,23 +339,23 @@ __device__ __forceinline__ void face_lookup(float e, float top, const float4* __
         const float4 q = __ldg(quads + (size_t)(last - 1) * TILE2);
         const float a1 = q.z;
         const float a0 = q.x;
-        const float c = (m - 1.0f) / m;
-        W = (a1 - a0) / (top * (1.0f - c * c));
+        const float c = qdiv(m - 1.0f, m);
+        W = qdiv(a1 - a0, top * (1.0f - c * c));
         A = a1 + W * (e - top);
-        T = q.w * (A / fmax32(a1, 1e-12f));
+        T = q.w * qdiv(A, fmax32(a1, 1e-12f));
         return;
     }
-    const float s = sqrtf(e / top) * m;
+    const float s = qsqrt(qdiv(e, top)) * m;
     const int r = row_of(s, last);
-    const float c0 = (float)r / m;
-    const float c1 = (float)(r + 1) / m;
+    const float c0 = qdiv((float)r, m);
+    const float c1 = qdiv((float)(r + 1), m);
     const float e0 = c0 * c0 * top;
     const float de = (c1 * c1 - c0 * c0) * top;
-    const float f = (e - e0) / de;
+    const float f = qdiv(e - e0, de);
     const float4 q = __ldg(quads + (size_t)r * TILE2);
     A = q.x + f * (q.z - q.x);
     T = q.y + f * (q.w - q.y);
-    W = (q.z - q.x) / de;
+    W = qdiv(q.z - q.x, de);
 }
 
 // The tile holding NATIVE index k, and the tile-layout index of k's cell.

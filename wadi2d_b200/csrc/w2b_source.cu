@@ -4,10 +4,12 @@
 //
 // The rate restates wadi2d/forcing.py:667-683 per cell: excess = (E(P1) - E(P0)) / (1000 dt), with the SCS loss of
 // wadi2d/hydrology/losses.py:69-72 or the initial-and-constant loss of wadi2d_b200/forcing.py; the window's rain
-// volume is the sum of the float32 rates times the cell area in FP64, times dt. Storage restates
+// volume is the sum of the float32 rates times the cell area in FP64, times dt. The lumped inflows restate the inflow
+// part of wadi2d/forcing.py:684-694 with the depths read in place. Storage restates
 // wadi2d/engine/monitor.py:214-218 (h + res over the interior cells, FP64). Each cell is weighed by the area of its
 // run's cells and its mean depth read from its run's current half, so one call serves a batch of runs as well.
 #include <cstdio>
+#include <cstring>
 
 #include "w2b_common.cuh"
 
@@ -93,6 +95,122 @@ __global__ void __launch_bounds__(SRC_THREADS) source_runs_kernel(StepArgs A, in
     }
 }
 
+// numpy's pairwise summation of n doubles (np.add.reduce on a contiguous float64 array, numpy's pairwise_sum): fewer
+// than 8 terms added in order from 0; up to 128 in eight interleaved partial sums combined as ((r0 + r1) + (r2 + r3)) +
+// ((r4 + r5) + (r6 + r7)), then the tail in order; beyond 128 the two halves (the first a multiple of 8 long) summed
+// so and added. Restated so that a device sum rounds as the host's np.sum does. Recursion unrolled with a stack.
+__device__ double pairwise_sum(const double* a, int n) {
+    struct Span {
+        int at, n, state;
+        double left;
+    };
+    Span stack[32];
+    int top = 0;
+    stack[0] = {0, n, 0, 0.0};
+    double ret = 0.0;
+    while (top >= 0) {
+        Span& sp = stack[top];
+        if (sp.n <= 128) {
+            double res;
+            const double* x = a + sp.at;
+            if (sp.n < 8) {
+                res = 0.0;
+                for (int i = 0; i < sp.n; ++i) res += x[i];
+            } else {
+                double r[8];
+                for (int j = 0; j < 8; ++j) r[j] = x[j];
+                int i = 8;
+                for (; i < sp.n - (sp.n % 8); i += 8)
+                    for (int j = 0; j < 8; ++j) r[j] += x[i + j];
+                res = ((r[0] + r[1]) + (r[2] + r[3])) + ((r[4] + r[5]) + (r[6] + r[7]));
+                for (; i < sp.n; ++i) res += x[i];
+            }
+            ret = res;
+            --top;
+            continue;
+        }
+        int n2 = sp.n / 2;
+        n2 -= n2 % 8;
+        if (sp.state == 0) {  // the first half
+            sp.state = 1;
+            stack[top + 1] = {sp.at, n2, 0, 0.0};
+            ++top;
+        } else if (sp.state == 1) {  // the first half's sum came back: now the second
+            sp.left = ret;
+            sp.state = 2;
+            stack[top + 1] = {sp.at + n2, sp.n - n2, 0, 0.0};
+            ++top;
+        } else {
+            ret = sp.left + ret;
+            --top;
+        }
+    }
+    return ret;
+}
+
+// The lumped inflows of a source window (wadi2d/forcing.py:684-694), in the host's order, one CTA: first every
+// injection cell's source is reset to the window's rain rate where the rain pass wrote one (else 0); then injection
+// by injection, those with a positive mean flow q share it over their cells (Injection.share,
+// wadi2d/forcing.py:468-476): by the level d read in place where d >= the injection's minimum depth, all to its
+// lowest cell while none is, the weights summed as np.sum sums them; each cell's float32 rate (q share / area) is
+// added to src as the host adds it; the injection's window volume is the float32 rates summed in FP64 (np.sum's
+// order) times the area and the window, and the window's total is added to volume[n].
+// The per-injection numbers of a window, by value: the mean flows, the cell ranges, the lowest cells and the depth
+// floors (all checked on the host).
+struct InflowArgs {
+    int32_t n, start[W2B_INFLOWS_MAX + 1], lowest[W2B_INFLOWS_MAX];
+    double q[W2B_INFLOWS_MAX], min_depth[W2B_INFLOWS_MAX];
+    double area;
+    const int32_t* cells;
+    const uint8_t* rained;
+    double* volume;
+};
+
+__global__ void __launch_bounds__(256) inflow_kernel(StepArgs A, InflowArgs F, double step) {
+    __shared__ double w[W2B_INFLOW_CELLS_MAX];
+    float* src = const_cast<float*>(A.src);
+    const int tid = threadIdx.x;
+    const int all = F.start[F.n];
+    for (int j = tid; j < all; j += blockDim.x) {
+        const int k = F.cells[j];
+        if (!F.rained[j]) src[k] = 0.0f;
+    }
+    __syncthreads();
+    double total = 0.0;
+    for (int i = 0; i < F.n; ++i) {
+        const double q = F.q[i];
+        const int s = F.start[i], m = F.start[i + 1] - s;
+        if (!(q > 0.0)) {
+            if (tid == 0) F.volume[i] = 0.0;
+            continue;
+        }
+        const double floor_depth = F.min_depth[i];
+        int wet = 0;
+        for (int j = tid; j < m; j += blockDim.x) {
+            const double dj = (double)A.d[F.cells[s + j]];
+            const bool on = dj >= floor_depth;
+            w[j] = on ? dj : 0.0;
+            wet |= on;
+        }
+        wet = __syncthreads_or(wet);
+        if (tid == 0) {
+            const double sum = wet ? pairwise_sum(w, m) : 0.0;
+            for (int j = 0; j < m; ++j) {
+                const double share = wet ? w[j] / sum : (j == F.lowest[i] ? 1.0 : 0.0);
+                const float rate = (float)(q * share / F.area);
+                const int k = F.cells[s + j];
+                src[k] = src[k] + rate;
+                w[j] = (double)rate;
+            }
+            const double vol = pairwise_sum(w, m) * F.area * step;
+            F.volume[i] = vol;
+            total += vol;
+        }
+        __syncthreads();
+    }
+    if (tid == 0) F.volume[F.n] += total;
+}
+
 // out[0] = scale * (sum of the partials, in order)
 __global__ void __launch_bounds__(SRC_THREADS) finish_kernel(const double* __restrict__ partial, int n, double scale,
                                                              double* __restrict__ out) {
@@ -136,6 +254,40 @@ int32_t w2b_source_runs(void* handle, int64_t n, const int32_t* cells, const flo
     const cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) {
         fprintf(stderr, "libwadi_b200: w2b_source_runs: %s\n", cudaGetErrorString(e));
+        return W2B_ECUDA;
+    }
+    return W2B_OK;
+}
+
+int32_t w2b_inflow_window(void* handle, const W2BInflow* inflow, const double* q, double t0, double t1,
+                          void* stream) {
+    if (!handle || !inflow || !(t1 > t0) || inflow->n < 0 || inflow->n > W2B_INFLOWS_MAX || (inflow->n && !q) ||
+        !inflow->volume || !(inflow->area > 0.0) ||
+        (inflow->n && (!inflow->start || !inflow->cells || !inflow->lowest || !inflow->min_depth || !inflow->rained)))
+        return W2B_EINVAL;
+    InflowArgs F;
+    memset(&F, 0, sizeof(F));
+    F.n = inflow->n;
+    F.area = inflow->area;
+    F.cells = inflow->cells;
+    F.rained = inflow->rained;
+    F.volume = inflow->volume;
+    if (F.n && inflow->start[0] != 0) return W2B_EINVAL;
+    for (int i = 0; i < F.n; ++i) {
+        const int m = inflow->start[i + 1] - inflow->start[i];
+        if (m < 1 || m > W2B_INFLOW_CELLS_MAX || inflow->lowest[i] < 0 || inflow->lowest[i] >= m) return W2B_EINVAL;
+        F.start[i] = inflow->start[i];
+        F.lowest[i] = inflow->lowest[i];
+        F.q[i] = q[i];
+        F.min_depth[i] = inflow->min_depth[i];
+    }
+    F.start[F.n] = F.n ? inflow->start[F.n] : 0;
+    StepArgs A;
+    if (!handle_args(handle, &A)) return W2B_EINVAL;
+    inflow_kernel<<<1, 256, 0, (cudaStream_t)stream>>>(A, F, t1 - t0);
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        fprintf(stderr, "libwadi_b200: w2b_inflow_window: %s\n", cudaGetErrorString(e));
         return W2B_ECUDA;
     }
     return W2B_OK;

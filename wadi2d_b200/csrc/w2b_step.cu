@@ -17,6 +17,17 @@
 
 namespace w2b {
 
+// The face and update passes are compiled twice (wadi2d_b200/build.py): into namespace exact with the library's IEEE
+// flags, the reference's float32 bits, and into namespace fast with W2B_FAST and FMA contraction (the approximate
+// division, square root and cube root of w2b_common.cuh qdiv/qsqrt/qcbrt). W2BParams.arith picks one per handle.
+// Everything after them (envelope, boundary, control, converters) is compiled once, with the exact build.
+#ifdef W2B_FAST
+#define W2B_ARITH fast
+#else
+#define W2B_ARITH exact
+#endif
+namespace W2B_ARITH {
+
 // ------------------------------------------------------------------ face pass
 
 // Shared-memory image of one tile for the face pass. Boxes of 40 x 36 floats hold the tile with 2 cells of halo north
@@ -78,14 +89,14 @@ __device__ __forceinline__ void face_a(const float* sm, int b, int local, const 
         const float* ZC = sm + (AX == 0 ? F_ZCX : F_ZCY) * BOX;
         const float dz = from_left ? ZC[b - S] - st[0 * TILE2 + local] : ZC[b] - st[1 * TILE2 + local];
         if (dz > 1e-6f) {
-            float phi = (eup - 2.0f * dz) / (2.0f * dz);
+            float phi = qdiv(eup - 2.0f * dz, 2.0f * dz);
             phi = phi < 0.0f ? 0.0f : (phi > 1.0f ? 1.0f : phi);
             eface = eup - phi * dz;
         }
     }
     const int last = A.rows - 1;
     const bool above = eface >= top;
-    const int r = above ? last - 1 : row_of(sqrtf(eface / top) * (float)last, last);
+    const int r = above ? last - 1 : row_of(qsqrt(qdiv(eface, top)) * (float)last, last);
     F.eface = eface;
     F.bits |= FA_LIVE | (above ? FA_ABOVE : 0) | r;
     const float4* quads = A.ftab4[AX] + (size_t)t * (A.rows - 1) * TILE2 + local;
@@ -165,14 +176,25 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
     const float us_s = ustar(ps ? u_s : uf, ps ? uss : u_n, ps ? uf : u_s, second);
     const float us_n = ustar(pn ? uf : u_n, pn ? u_s : unn, pn ? u_n : uf, second);
     flux += qy_n * us_n - qy_s * us_s;
-    // [4] momentum and pressure
+    // [4] momentum and pressure (the fast build multiplies by one reciprocal of the span, which the compiler hoists
+    // out of the tile's loop)
     const float abar = HALF * (h_l + h_r) * dx;
-    const float press = dt * P.g * d_eta / span;
+#ifdef W2B_FAST
+    const float rspan = __fdividef(ONE, span);
+    const float press = dt * P.g * d_eta * rspan;
     float us;
     if (abar > 1e-6f * dx)
-        us = (sm[SM_M + AX * TILE2 + local] - dt * flux / span) / abar - press;
+        us = qdiv(sm[SM_M + AX * TILE2 + local] - dt * flux * rspan, abar) - press;
     else
         us = uf - press;
+#else
+    const float press = qdiv(dt * P.g * d_eta, span);
+    float us;
+    if (abar > 1e-6f * dx)
+        us = qdiv(sm[SM_M + AX * TILE2 + local] - qdiv(dt * flux, span), abar) - press;
+    else
+        us = uf - press;
+#endif
     const float vb = 0.25f * (VP[b - S] + VP[b] + VP[b - S + PP] + VP[b + PP]);
 
     // the table lookup from the quad loaded in part A (common.cuh face_lookup); rowc holds, per row r, c0^2 and
@@ -183,36 +205,50 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
     float area, tt, w;
     if (F.bits & FA_ABOVE) {
         const float a1 = q.z, a0 = q.x;
-        w = (a1 - a0) / (top * rowc[2 * (A.rows - 1)]);
+        w = qdiv(a1 - a0, top * rowc[2 * (A.rows - 1)]);
         area = a1 + w * (e - top);
-        tt = q.w * (area / fmax32(a1, 1e-12f));
+        tt = q.w * qdiv(area, fmax32(a1, 1e-12f));
     } else {
         const int r = F.bits & FA_ROW;
         const float e0 = rowc[2 * r] * top;
         const float de = rowc[2 * r + 1] * top;
-        const float f = (e - e0) / de;
+#ifdef W2B_FAST
+        const float rde = __fdividef(ONE, de);  // one reciprocal for both quotients
+        const float f = (e - e0) * rde;
         area = q.x + f * (q.z - q.x);
         tt = q.y + f * (q.w - q.y);
-        w = (q.z - q.x) / de;
+        w = (q.z - q.x) * rde;
+#else
+        const float f = qdiv(e - e0, de);
+        area = q.x + f * (q.z - q.x);
+        tt = q.y + f * (q.w - q.y);
+        w = qdiv(q.z - q.x, de);
+#endif
     }
     // [1] the volume-limited section
     float rho = ONE;
     if (P.sheet) {
         const float avol = hup * dx;
         if (avol < area) {
-            const float sub = fmin32(I.e_lp, I.e_rp) / fmax32(I.e_lp, I.e_rp);
+            const float sub = qdiv(fmin32(I.e_lp, I.e_rp), fmax32(I.e_lp, I.e_rp));
             const float sub2 = sub * sub;
             const float alpha = sub2 * sub2;
-            rho = alpha + (ONE - alpha) * avol / area;
+            rho = alpha + qdiv((ONE - alpha) * avol, area);
         }
     }
-    // [5] friction
-    const float t3 = tt * tt * tt * cbrt32(tt);
-    float fric = area * area / fmax32(t3, 1e-30f);
-    if (rho < ONE) fric = fric / fmax32(rho * cbrt32(rho), 1e-12f);
+    // [5] friction. The fast build forms 1 / max(tt^(10/3), 1e-30) and 1 / max(rho^(4/3), 1e-12) as capped powers from
+    // the hardware log2 and exp2 (within about 1e-6 relative; tt = 0 or rho = 0 gives the cap, as the clamps do).
+#ifdef W2B_FAST
+    float fric = area * area * fmin32(ex2_approx(-3.33333325f * lg2_approx(tt)), 1e30f);
+    if (rho < ONE) fric = fric * fmin32(ex2_approx(-1.33333337f * lg2_approx(rho)), 1e12f);
+#else
+    const float t3 = tt * tt * tt * qcbrt(tt);
+    float fric = qdiv(area * area, fmax32(t3, 1e-30f));
+    if (rho < ONE) fric = qdiv(fric, fmax32(rho * qcbrt(rho), 1e-12f));
+#endif
     const float a = dt * P.g * fric;
-    const float sp = sqrtf(us * us + vb * vb);
-    float un = 2.0f * us / (ONE + sqrtf(ONE + 4.0f * a * sp));
+    const float sp = qsqrt(us * us + vb * vb);
+    float un = qdiv(2.0f * us, ONE + qsqrt(ONE + 4.0f * a * sp));
     if (fabsf(un) > P.u_max) un = un > ZERO ? P.u_max : -P.u_max;
     // [6] crest face
     float qn = area * rho * un;
@@ -224,12 +260,12 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
             const float ua = from_left ? um : up;
             float tc;
             const float4* quads = A.ftab4[AX] + (size_t)t * (A.rows - 1) * TILE2 + local;
-            face_lookup(eup + HALF * ua * ua / P.g, top, quads, A.rows, area_c, tc, w_c);
+            face_lookup(eup + qdiv(HALF * ua * ua, P.g), top, quads, A.rows, area_c, tc, w_c);
         }
-        const float qc = c * area_c * sqrtf(area_c / fmax32(w_c, 1e-9f));
+        const float qc = c * area_c * qsqrt(qdiv(area_c, fmax32(w_c, 1e-9f)));
         if (fabsf(qn) > qc) {
             qn = qn > ZERO ? qc : -qc;
-            un = qn / fmax32(area * rho, 1e-12f);
+            un = qdiv(qn, fmax32(area * rho, 1e-12f));
         }
     }
     if constexpr (PROBE) {
@@ -249,7 +285,7 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
     float plan = from_left ? OM[b - S] : OM[b];
     const float dother = from_left ? d_right : d_left;
     if (dother > P.h_cfl) plan = fmin32(plan, from_left ? OM[b] : OM[b - S]);
-    const float wave = sqrtf(fmax32(P.g * area * rho / (fmax32(plan, P.a_min) * dx), ZERO));
+    const float wave = qsqrt(fmax32(qdiv(P.g * area * rho, fmax32(plan, P.a_min) * dx), ZERO));
     return fabsf(un) + fmin32(P.lead * fabsf(un - uf), 2.0f * wave) + wave;
 }
 
@@ -371,43 +407,6 @@ __global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_co
         }
     }
 }
-
-// Every positive float from first (as bits) on: cbrt32 against the double path; out[0] counts mismatches,
-// out[1..4] keep some mismatching inputs.
-__global__ void cbrt_check_kernel(uint32_t first, uint32_t count, unsigned long long* out) {
-    for (uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; n < count; n += (uint64_t)gridDim.x * blockDim.x) {
-        const uint32_t bits = first + (uint32_t)n;
-        const float x = __uint_as_float(bits);
-        const float a = cbrt32(x);
-        const float b = (float)cbrt((double)x);
-        if (__float_as_uint(a) != __float_as_uint(b) && !(isnan(a) && isnan(b))) {
-            const unsigned long long k = atomicAdd(out, 1ull);
-            if (k < 4) out[1 + k] = bits;
-        }
-    }
-}
-
-void launch_cbrt_check(uint32_t first, uint32_t count, unsigned long long* out, cudaStream_t s) {
-    cbrt_check_kernel<<<148 * 16, 256, 0, s>>>(first, count, out);
-}
-
-// The bounded wait's give-up path, run on purpose: thread 0 arms a barrier for 16 bytes that no copy will bring, so
-// its phase cannot complete, and waits on it with mbar_wait for `polls` polls. Nothing is in flight, so the CTA may
-// leave. out[0] = W2B_ETIMEOUT if the wait gave up (W2B_OK if it completed, which it cannot), out[1] = the clock
-// cycles the wait took.
-__global__ void wait_check_kernel(uint32_t polls, long long* out) {
-    __shared__ __align__(8) uint64_t bar;
-    if (threadIdx.x != 0) return;
-    mbar_init(&bar, 1);
-    fence_barrier_init();
-    mbar_expect_tx(&bar, 16);  // the one arrival, with 16 bytes still expected
-    const long long t0 = clock64();
-    const bool ok = mbar_wait(&bar, 0, polls);
-    out[1] = clock64() - t0;
-    out[0] = ok ? W2B_OK : W2B_ETIMEOUT;
-}
-
-void launch_wait_check(uint32_t polls, long long* out, cudaStream_t s) { wait_check_kernel<<<1, 32, 0, s>>>(polls, out); }
 
 // The wave speed and the new velocity of every own face of tile t for a step dt from the current state, as the face
 // pass would compute them, written to out ([wx | wy | un_x | un_y], 1024 each, tile layout) and nothing else: the
@@ -670,6 +669,48 @@ int update_occupancy() {
 void launch_update(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s) {
     update_kernel<<<grid, dim3(32, 8), UPDATE_SMEM, s>>>(M, A);
 }
+
+}  // namespace W2B_ARITH
+
+#ifndef W2B_FAST
+// ------------------------------------------------------------------ self-checks
+
+// Every positive float from first (as bits) on: cbrt32 against the double path; out[0] counts mismatches,
+// out[1..4] keep some mismatching inputs.
+__global__ void cbrt_check_kernel(uint32_t first, uint32_t count, unsigned long long* out) {
+    for (uint64_t n = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; n < count; n += (uint64_t)gridDim.x * blockDim.x) {
+        const uint32_t bits = first + (uint32_t)n;
+        const float x = __uint_as_float(bits);
+        const float a = cbrt32(x);
+        const float b = (float)cbrt((double)x);
+        if (__float_as_uint(a) != __float_as_uint(b) && !(isnan(a) && isnan(b))) {
+            const unsigned long long k = atomicAdd(out, 1ull);
+            if (k < 4) out[1 + k] = bits;
+        }
+    }
+}
+
+void launch_cbrt_check(uint32_t first, uint32_t count, unsigned long long* out, cudaStream_t s) {
+    cbrt_check_kernel<<<148 * 16, 256, 0, s>>>(first, count, out);
+}
+
+// The bounded wait's give-up path, run on purpose: thread 0 arms a barrier for 16 bytes that no copy will bring, so
+// its phase cannot complete, and waits on it with mbar_wait for `polls` polls. Nothing is in flight, so the CTA may
+// leave. out[0] = W2B_ETIMEOUT if the wait gave up (W2B_OK if it completed, which it cannot), out[1] = the clock
+// cycles the wait took.
+__global__ void wait_check_kernel(uint32_t polls, long long* out) {
+    __shared__ __align__(8) uint64_t bar;
+    if (threadIdx.x != 0) return;
+    mbar_init(&bar, 1);
+    fence_barrier_init();
+    mbar_expect_tx(&bar, 16);  // the one arrival, with 16 bytes still expected
+    const long long t0 = clock64();
+    const bool ok = mbar_wait(&bar, 0, polls);
+    out[1] = clock64() - t0;
+    out[0] = ok ? W2B_OK : W2B_ETIMEOUT;
+}
+
+void launch_wait_check(uint32_t polls, long long* out, cudaStream_t s) { wait_check_kernel<<<1, 32, 0, s>>>(polls, out); }
 
 // ------------------------------------------------------------------ envelope pass
 
@@ -1087,5 +1128,7 @@ __global__ void bmark_kernel(StepArgs A, int clear_words) {
         atomicOr(mark + fid / TILE, 1u << (fid % TILE));
     }
 }
+
+#endif  // W2B_FAST
 
 }  // namespace w2b

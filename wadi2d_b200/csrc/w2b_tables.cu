@@ -448,6 +448,7 @@ int32_t w2b_build_tables(const W2BTableIn* in, const W2BTableOut* out, void* str
         in->rows > ROWS_MAX || in->ntiles < 1 || in->ny % TILE || in->nx % TILE || in->zh < 1 || in->zw < 1)
         return W2B_EINVAL;
     if (in->local && (!out->ws || out->ws_threads < 1)) return W2B_EINVAL;
+    if (in->local && (in->margin < 0 || in->margin > W2B_TABLE_MARGIN_MAX)) return W2B_EINVAL;
     TableArgs A;
     A.z = in->z;
     A.zh = in->zh;
@@ -558,9 +559,9 @@ int32_t w2b_build_tables(const W2BTableIn* in, const W2BTableOut* out, void* str
 constexpr size_t NOALLOC_SCRATCH_BYTES = (size_t)32 << 20;
 static __device__ __align__(256) double noalloc_scratch[NOALLOC_SCRATCH_BYTES / sizeof(double)];
 
-// The array's device address, looked up once per device with that device current. In host code the name
-// noalloc_scratch is a host-side stand-in, not a device address: a kernel given it would fault or read the wrong
-// memory, so only this address is ever passed on.
+// The array's device address, looked up once per device with that device current and kept for the life of the
+// process (a cudaDeviceReset makes it stale). In host code the name noalloc_scratch is a host-side stand-in, not a
+// device address: a kernel given it would fault or read the wrong memory, so only this address is ever passed on.
 static std::mutex noalloc_mutex;
 static void* noalloc_address[256];
 
@@ -584,18 +585,18 @@ static int noalloc_scratch_address(void** out) {
 
 extern "C" int32_t w2b_build_tables_noalloc(const W2BTableIn* in, const W2BTableOut* out, void* stream) {
     if (!in || !out) return W2B_EINVAL;
+    if (in->local && (in->margin < 0 || in->margin > W2B_TABLE_MARGIN_MAX)) return W2B_EINVAL;
     W2BTableOut o = *out;
     o.ws = nullptr;
     o.ws_threads = 0;
     if (in->local) {
-        const int margin = in->margin > 0 ? in->margin : 0;
-        const int64_t per_thread = 9 * (int64_t)(in->k + 2 * margin + 1) * (int64_t)sizeof(double);
+        const int64_t per_thread = 9 * ((int64_t)in->k + 2 * (int64_t)in->margin + 1) * (int64_t)sizeof(double);
         const int64_t threads = (int64_t)(NOALLOC_SCRATCH_BYTES / (size_t)per_thread) / 128 * 128;
         if (threads < 128) {
             fprintf(stderr,
                     "libwadi_b200: w2b_build_tables_noalloc: face lines of %d pixels need %lld bytes of scratch for "
                     "128 threads; the static scratch holds %zu (at most %lld pixels a line)\n",
-                    in->k + 2 * margin, (long long)(per_thread * 128), NOALLOC_SCRATCH_BYTES,
+                    in->k + 2 * in->margin, (long long)(per_thread * 128), NOALLOC_SCRATCH_BYTES,
                     (long long)(NOALLOC_SCRATCH_BYTES / (128 * 9 * sizeof(double)) - 1));
             return W2B_EINVAL;
         }

@@ -4,7 +4,9 @@ books are kept as the reference's monitor keeps them (wadi2d/engine/monitor.py:3
 
 Rain comes either from the host (``forcing.Forcing.rate``, the reference's form: a float32 rate per interior cell
 uploaded each window) or from the device (``DeviceRain``: the same rate formed on the GPU from per-cell storm depth
-multipliers, which removes the per-window upload).
+multipliers, which removes the per-window upload). Lumped inflows likewise: on the host (``Forcing`` with
+injections, the cells' levels read back from the device each window) or on the device (``DeviceInflow``: each
+hydrograph's window flow shared by the levels read in place, no read-back and no upload).
 """
 
 from __future__ import annotations
@@ -67,6 +69,50 @@ class DeviceRain:
         return float(self.volume.item())
 
 
+class DeviceInflow:
+    """Lumped inflows rated on the device each window (w2b_inflow_window): each injection's mean flow over the
+    window (the exact integral of its piecewise-linear hydrograph, ``forcing.Injection.mean_flow``, on the host) is
+    shared over its cells by their level, read in place on the device, as ``forcing.Forcing.rate`` shares it on the
+    host (wadi2d/forcing.py:684-694, :468-476). ``rained``: reference state indices of the cells whose source the
+    window's ``DeviceRain`` writes (the inflow is added on top of their rain), or None. The window volumes are kept on
+    the device; ``total()`` reads their sum once."""
+
+    def __init__(self, model, injections, area: float, rained=None) -> None:
+        b = model.backend
+        torch = b.torch
+        self.model, self.injections = model, list(injections)
+        n = len(self.injections)
+        if n > _lib.INFLOWS_MAX:
+            raise ValueError(f"{n} inflows: at most {_lib.INFLOWS_MAX} a call")
+        index = [np.asarray(inj.index, np.int64) for inj in self.injections]
+        self.start = np.concatenate(([0], np.cumsum([i.size for i in index]))).astype(np.int32)
+        allidx = np.concatenate(index) if n else np.zeros(0, np.int64)
+        native = native_of_ref(model.grid.tiles, allidx, model.grid.shape[1]).astype(np.int32)
+        flags = np.zeros(allidx.size, np.uint8) if rained is None else np.isin(allidx, rained).astype(np.uint8)
+        self.cells = torch.as_tensor(native, device=b.device)
+        self.rained = torch.as_tensor(flags, device=b.device)
+        self.lowest = np.array([inj.lowest for inj in self.injections], np.int32)
+        self.min_depth = np.array([inj.min_depth for inj in self.injections], np.float64)
+        self.volume = torch.zeros(n + 1, dtype=torch.float64, device=b.device)
+        self.tiles = [np.unique(i // 1296) for i in index]
+        self.arg = _lib.Inflow(n, self.start.ctypes.data, self.lowest.ctypes.data, self.min_depth.ctypes.data,
+                               self.cells.data_ptr(), self.rained.data_ptr(), float(area),
+                               self.volume.data_ptr())  # fmt: skip
+
+    def window(self, t0: float, t1: float) -> np.ndarray:
+        """Add the window's inflow rates to src on the device; return the tiles of the injections that flow in it."""
+        q = np.array([inj.mean_flow(t0, t1) for inj in self.injections], np.float64)
+        b = self.model.backend
+        _lib.call("w2b_inflow_window", b.handle, ctypes.byref(self.arg), q.ctypes.data, float(t0), float(t1),
+                  b._stream())  # fmt: skip
+        flowing = [self.tiles[i] for i in range(len(q)) if q[i] > 0.0]
+        return np.concatenate(flowing) if flowing else np.zeros(0, np.int64)
+
+    def total(self) -> float:
+        """The inflow volume of every window so far, m3 (FP64, summed as the host form sums it)."""
+        return float(self.volume[len(self.injections)].item())
+
+
 class DeviceStorage:
     """FP64 storage (h + res) over a set of cells, on the device (w2b_storage)."""
 
@@ -95,9 +141,10 @@ class RunSummary:
 
 
 def run_windows(model, t_end: float, rain=None, host_forcing=None, window: float = 30.0, maxima=None, tally=None,
-                storage=None, on_window=None) -> RunSummary:  # fmt: skip
-    """Advance ``model`` to ``t_end`` window by window; rain from ``rain`` (DeviceRain) or ``host_forcing``
-    (forcing.Forcing, whose ``state`` are the interior cells)."""
+                storage=None, on_window=None, inflow=None) -> RunSummary:  # fmt: skip
+    """Advance ``model`` to ``t_end`` window by window; rain from ``rain`` (DeviceRain) and lumped inflows from
+    ``inflow`` (DeviceInflow), or both from ``host_forcing`` (forcing.Forcing, whose ``state`` are the interior
+    cells)."""
     bal = Balance()
     if storage is not None:
         bal.storage0 = bal.storage = storage()
@@ -106,16 +153,23 @@ def run_windows(model, t_end: float, rain=None, host_forcing=None, window: float
     windows = 0
     while t < t_end - 1e-9:
         t1 = min(t + window, t_end)
-        if rain is not None:
-            bal.rain += rain.window(t, t1)
-            st = model.stepper
-            if st.adaptive_active:  # as set_source_cells does: rained tiles stay active while rain falls
+        if rain is not None or inflow is not None:
+            falling = False
+            if rain is not None:
+                bal.rain += rain.window(t, t1)
                 falling = rain.storm.cumulative_depth(np.array([t1 / 60.0]))[0] > rain.storm.cumulative_depth(
                     np.array([t / 60.0]))[0]
-                st.keep_active[:] = False
-                if falling:
-                    st.keep_active[rain.tiles] = True
-                st.keep_active[model.boundary_tiles] = True
+            flowing = inflow.window(t, t1) if inflow is not None else None
+            st = model.stepper
+            # as set_source_cells does: tiles that take a source stay active while it runs (an injection's tiles
+            # whole, a superset of its cells with a nonzero rate: a dry tile stepped is left as it was)
+            st.keep_active[:] = False
+            if falling:
+                st.keep_active[rain.tiles] = True
+            if flowing is not None and flowing.size:
+                st.keep_active[flowing] = True
+            st.keep_active[model.boundary_tiles] = True
+            if st.adaptive_active:
                 st.rebuild_active(retain=True)
             st.refresh_due = True
         elif host_forcing is not None:
@@ -128,6 +182,8 @@ def run_windows(model, t_end: float, rain=None, host_forcing=None, window: float
         windows += 1
         if on_window is not None:
             on_window(t, bal)
+    if inflow is not None:
+        bal.inflow = inflow.total()
     if tally is not None:
         bal.outflow = tally.volume()
     if storage is not None:

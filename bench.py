@@ -47,7 +47,7 @@ FALLBACK_HBM_GBS = 6650.0
 # (1,115,136 tile cells, beyond L2); the traffic grows with the tile cells a launch processes, so it scales to this
 # launch by them.
 FACES_DRAM_BYTES_PER_CELL = 178.6
-CPU_BLOCK_TILES = 32  # the CPU sample: a 32 x 32-tile block (1,048,576 cells) from the middle of the grid
+CPU_BLOCK_TILES = 32  # the CPU sample: a 32 x 32-tile block (1,044,484 active cells) from the middle of the grid
 
 
 def parse():
@@ -202,14 +202,16 @@ def cpu_block(grid) -> tuple[int, int, int]:
 
 
 def block_inputs(c, grid, rate):
-    """The CPU sample block as the reference's CPU path takes it: the oracle's grid of the block (every cell active,
-    walls on its edge), its tables from the oracle's table builder (the reference's builder restated) on the block's
+    """The CPU sample block as the reference's CPU path takes it: the oracle's grid of the block (every cell active but
+    the outer ring, walls on its edge), its tables from the oracle's table builder (the reference's builder restated) on the block's
     own pixels (``c.block_z``, cut from the catchment's bed; faces at the block's edge see the block's pixels), and the
     source rates of the block's cells."""
     from oracle import oracle as O
 
     j0, i0, M = cpu_block(grid)
-    og = O.Grid(0.0, 0.0, grid.dx, np.ones((M, M), bool))
+    # the reference's padded grid of the block (wadi2d/grid/tiles.py:52-64): its outer ring of cells inactive, so every
+    # face at the block's edge is closed, as on any grid the reference builds
+    og = O.Grid.from_mask(np.ones((M - 2, M - 2), bool), 0.0, 0.0, grid.dx)
     tables = O.build_tables(og, c.block_z, c.dx / c.k, c.manning, local_radius=True)
     return og, tables, rate[j0 : j0 + M, i0 : i0 + M]
 
@@ -226,7 +228,7 @@ def cpu_sample(block, seconds: float, threads: int, steps: int | None = None, wa
     m.adaptive_active = False
     m.set_depth(np.full(og.mask.shape, 0.05))
     m.set_source(rate)
-    cells = og.mask.size
+    cells = int(og.mask.sum())
     for _ in range(warmup):
         m.advance(m.t + m.dt * 0.999)
     n0, t0 = m.nsteps, time.perf_counter()
@@ -271,7 +273,7 @@ def block_parity(block, arith: str, steps: int, threads: int) -> dict:
     O.threads(threads)
     ref = O.Model(og, tables, O.Numerics())
     ref.adaptive_active = False
-    grid = TileGrid(0.0, 0.0, og.dx, og.mask)
+    grid = TileGrid(og.x0, og.y0, og.dx, og.mask)
     m = Model(GridTables.from_dict(grid, tables), Numerics(arithmetic=arith))
     m.stepper.adaptive_active = False
     dts = []
@@ -286,7 +288,7 @@ def block_parity(block, arith: str, steps: int, threads: int) -> dict:
         model.set_depth(np.full(og.mask.shape, 0.05))
         model.set_source(rate)
         _steps(model, steps)
-    out = {"arith": arith, "steps": int(m.stepper.nsteps), "cells": int(og.mask.size),
+    out = {"arith": arith, "steps": int(m.stepper.nsteps), "cells": int(og.mask.sum()),
            "dt_identical": dts == [float(x) for x in ref.dts],
            "dt_max_rel_diff": float(np.max(np.abs(np.array(dts) / np.array(ref.dts) - 1.0))) if dts else 0.0}  # fmt: skip
     f = {n: (m.field(n), ref.field(n)) for n in ("h", "d", "u", "v", "mx", "my", "qx", "qy", "res", "om")}
@@ -933,6 +935,7 @@ def main() -> None:
     storage = DeviceStorage(m, np.asarray(state_index(grid, jj, ii), np.int64))
     del jj, ii
     src_native = b.native("src").cpu().pin_memory()
+    env_host = [torch.empty(a.shape, dtype=a.dtype).pin_memory() for a in maxima.arrays]  # the maps' host buffers
     win = 30.0
     h2d = d2h = 0
     torch.cuda.synchronize(dev)
@@ -947,8 +950,9 @@ def main() -> None:
         d2h += ctypes.sizeof(_lib.Clock) + 4 * (int(b.nact) + grid.ntiles)  # the clock, the active list, idle counts
         series.append((m.stepper.t, float(line.discharge()[0]), tally.volume(), storage()))
         d2h += 8 * 3
-    env = [a.cpu() for a in maxima.arrays]
-    d2h += sum(a.numel() * a.element_size() for a in env)
+    for dst, a in zip(env_host, maxima.arrays, strict=True):
+        dst.copy_(a, non_blocking=True)
+    d2h += sum(a.numel() * a.element_size() for a in env_host)
     torch.cuda.synchronize(dev)
     e2e_s = time.perf_counter() - w0
     e2e_steps = m.stepper.nsteps - s0
@@ -959,7 +963,7 @@ def main() -> None:
                         "the five envelope maps",
            "last_window": {"t_s": series[-1][0], "line_q_m3s": series[-1][1], "outflow_m3": series[-1][2],
                            "storage_m3": series[-1][3]} if series else None}  # fmt: skip
-    del env
+    del env_host
 
     wet_fraction = float((m.field("h") > 0).sum()) / cells
     launch = b.loop_config()

@@ -115,6 +115,11 @@ typedef struct {
     const int32_t *tile_run;
     /* staging for REF_TILE transfers: ntiles * 1296 floats */
     float *stage;
+    /* (ntiles) int32, or NULL: the tile of the static arrays (hc, the face scalars) and of the packed tables that each
+     * tile reads. NULL: every tile its own (the arrays have ntiles tiles). Runs of a batch on one catchment can share
+     * one copy: the arrays then hold only the distinct tiles (tile 0 the void tile), and table_tile maps each tile of
+     * the batch to its catchment tile. No counterpart in the reference, which copies the tables into every run. */
+    const int32_t *table_tile;
 } W2BBuffers;
 
 #define W2B_CTL_BYTES 1024

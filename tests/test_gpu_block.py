@@ -1,8 +1,8 @@
-"""Configuration 3 on the B200 against the oracle: the middle 32 x 32-tile block (1,048,576 cells) of the 4096 x 4096
-seeded catchment that bench.py times, its tables from the oracle's table builder on the block's own pixels, 0.05 m of
-water under the storm's peak rain, 200 steps of each's host-driven loop at the reference's dt rule
-(``bench.block_parity``, which the default bench line also reports). The exact build must be the oracle bit for bit,
-the fast build within the step's accuracy bounds."""
+"""Configuration 3 on the B200 against the oracle: the middle 32 x 32-tile block of the 4096 x 4096 seeded catchment
+that bench.py times (padded as the reference pads a grid: 1,044,484 active cells inside an inactive outer ring), its
+tables from the oracle's table builder on the block's own pixels, 0.05 m of water under the storm's peak rain, 200
+steps of each's host-driven loop at the reference's dt rule (``bench.block_parity``, which the default bench line also
+reports). The exact build must be the oracle bit for bit, the fast build within the step's accuracy bounds."""
 
 from __future__ import annotations
 

@@ -61,10 +61,9 @@ def _rough(amplitude, corr, seed, n_modes=256):
     return bed
 
 
-def _lake(bed_pixels, dx, k, level, arith):
-    """The oracle's tables of the bed, a product model on them (``arith`` build) and an oracle model, both at the
-    level through the tables."""
-    n = bed_pixels.shape[0] // k - 2
+def _lake(bed_pixels, n, dx, k, level, arith):
+    """The oracle's tables of the bed (n x n cells, padded), a product model on them (``arith`` build) and an oracle
+    model, both at the level through the tables."""
     og = O.Grid.from_mask(np.ones((n, n), bool), 0.0, 0.0, dx)
     tab = O.build_tables(og, bed_pixels, dx / k, 0.03, local_radius=True)
     grid = TileGrid(og.x0, og.y0, og.dx, og.mask)
@@ -87,7 +86,7 @@ def test_water_on_terraces_stays_exactly_still(arith, loop):
     rng = np.random.default_rng(1)
     cellz = 1500.0 + 0.125 * rng.integers(0, 9, size=(pad, pad))
     z = np.repeat(np.repeat(cellz, k, 0), k, 1)
-    m, _ = _lake(z, dx, k, 1500.5, arith)
+    m, _ = _lake(z, n, dx, k, 1500.5, arith)
     h0, d0 = m.field("h").copy(), m.field("d").copy()
     wet = int((h0 > 0).sum())
     assert 0.3 * n * n < wet < 0.8 * n * n
@@ -109,7 +108,7 @@ def test_rough_lake_at_rest_keeps_the_reference_round_off(arith):
     p = dx / k
     xs, ys = np.meshgrid((np.arange(pad * k) - k + 0.5) * p, (np.arange(pad * k) - k + 0.5) * p)
     z = _rough(0.5, 5.0 * dx, 0)(xs, ys) + lift
-    m, ref = _lake(z, dx, k, lift, arith)
+    m, ref = _lake(z, n, dx, k, lift, arith)
     h0 = m.field("h").astype(np.float64)
     v0 = m.volume()
     _steps(m, STEPS)

@@ -134,14 +134,18 @@ class B200Backend:
 
     name = "b200"
 
-    def __init__(self, tables: GridTables, num: NumericsRecord, device=None, tile_run=None, nruns: int = 1) -> None:
+    def __init__(self, tables: GridTables, num: NumericsRecord, device=None, tile_run=None, nruns: int = 1,
+                 grid=None, table_tile=None) -> None:  # fmt: skip
+        """``grid`` (default ``tables.grid``) is the grid stepped; with ``table_tile`` (one entry a tile of it) the
+        tables hold only distinct tiles and tile t reads table tile ``table_tile[t]`` (a batch's runs on one catchment
+        sharing one copy)."""
         import torch
 
         self.torch = torch
         if not torch.cuda.is_available():
             raise RuntimeError("B200Backend needs a CUDA device; this package has no CPU fallback")
         self.device = torch.device(device if device is not None else "cuda")
-        self.grid = tables.grid
+        self.grid = tables.grid if grid is None else grid
         self.num = num
         self.rows = tables.rows
         g = self.grid
@@ -181,9 +185,12 @@ class B200Backend:
         for ax in "xy":
             for f in ("fl", "fr", "gl", "gr", "ef", "cw"):
                 t[f + ax] = tab(f + ax)
-        t["dtab2"] = f32(nt * (rows - 1) * TILE2 * 2)
-        t["ftab4x"] = f32(nt * (rows - 1) * TILE2 * 4)
-        t["ftab4y"] = f32(nt * (rows - 1) * TILE2 * 4)
+        ntab = t["hc"].numel() // TILE2  # tiles of the static arrays: nt, or the distinct tiles under table_tile
+        if table_tile is None and ntab != nt:
+            raise ValueError(f"tables of {ntab} tiles for a grid of {nt}")
+        t["dtab2"] = f32(ntab * (rows - 1) * TILE2 * 2)
+        t["ftab4x"] = f32(ntab * (rows - 1) * TILE2 * 4)
+        t["ftab4y"] = f32(ntab * (rows - 1) * TILE2 * 4)
         t["tiles"] = up(g.tiles, torch.int32)
         t["tile_of"] = up(g.tile_of, torch.int32)
         t["nbr"] = up(g.nbr, torch.int32)
@@ -199,17 +206,28 @@ class B200Backend:
         t["tile_run"] = (torch.zeros(nt, dtype=torch.int32, device=dev) if tile_run is None
                          else torch.as_tensor(np.ascontiguousarray(tile_run, np.int32), device=dev))  # fmt: skip
         t["stage"] = f32(nt * STRIDE2)
+        if table_tile is not None:
+            tt = np.ascontiguousarray(table_tile, np.int32)
+            if tt.shape != (nt,) or tt.min() < 0 or tt.max() >= ntab or tt[0] != 0:
+                raise ValueError("table_tile: one entry a tile, in [0, table tiles), the void tile on tile 0")
+            t["table_tile"] = torch.as_tensor(tt, device=dev)
         self._t = t
         # own cells of every allocated tile, NATIVE index in tile-layout order (fid = t * 1024 + j * 32 + i)
         jj, ii = np.divmod(np.arange(TILE2), TILE)
         j = g.tiles[1:, 0, None].astype(np.int64) * TILE + jj[None, :]
         i = g.tiles[1:, 1, None].astype(np.int64) * TILE + ii[None, :]
         self._own = torch.as_tensor(((j + 4) * self.px + i + 32).reshape(-1), device=dev)
-        t["zcx"][self._own] = tab("zcx")[TILE2:]
-        t["zcy"][self._own] = tab("zcy")[TILE2:]
+        for zc in ("zcx", "zcy"):
+            z = tab(zc)
+            if table_tile is not None:
+                z = z.view(ntab, TILE2)[t["table_tile"][1:].long()].reshape(-1)
+            else:
+                z = z[TILE2:]
+            t[zc][self._own] = z
         dtab, fx, fy = tab("dtab"), tab("ftabx"), tab("ftaby")
         stream = self._stream()
-        _lib.call("w2b_pack_tables", ctypes.byref(self._desc), dtab.data_ptr(), fx.data_ptr(), fy.data_ptr(),
+        tab_desc = _lib.GridDesc(ny, nx, ntab, rows, self.nruns)
+        _lib.call("w2b_pack_tables", ctypes.byref(tab_desc), dtab.data_ptr(), fx.data_ptr(), fy.data_ptr(),
                   t["dtab2"].data_ptr(), t["ftab4x"].data_ptr(), t["ftab4y"].data_ptr(), stream)  # fmt: skip
         torch.cuda.current_stream(dev).synchronize()
         del dtab, fx, fy
@@ -228,6 +246,7 @@ class B200Backend:
             B.ftab4[a] = t["ftab4" + ax].data_ptr()
         for e in range(5):
             B.env[e] = t["env"][e].data_ptr()
+        B.table_tile = t["table_tile"].data_ptr() if "table_tile" in t else None
         self._buffers = B
         self._params = self._make_params(num)
         handle = ctypes.c_void_p()

@@ -135,18 +135,42 @@ class Batch:
         nt = grid.ntiles
         self.grid = grid
         dev = torch.device(device if device is not None else "cuda")
+        # runs given the same table object (one catchment under many storms) share one copy of it: the static arrays
+        # hold each distinct table set once, and every tile reads its set's tile (table_tile)
+        distinct: list = []
+        owner = []
+        for tab in tables:
+            u = next((k for k, v in enumerate(distinct) if v is tab), None)
+            if u is None:
+                u = len(distinct)
+                distinct.append(tab)
+            owner.append(u)
+        shared = len(distinct) < n
         arrays = {}
-        for f in TILE_FIELDS:
-            srcs = [self._table_array(tab, f, dev) for tab in tables]
-            a = torch.empty((nt,) + tuple(srcs[0].shape[1:]), dtype=srcs[0].dtype, device=dev)
-            a[0] = srcs[0][0]
-            for r, s in enumerate(srcs):
-                a.index_copy_(0, torch.as_tensor(self.map[r][1:], device=dev), s[1:])
-            arrays[f] = a
+        table_tile = None
+        if shared:
+            first = [owner.index(u) for u in range(len(distinct))]
+            offset = np.cumsum([1] + [grids[r].ntiles - 1 for r in first])
+            table_tile = np.zeros(nt, np.int32)
+            for r in range(n):
+                table_tile[self.map[r][1:]] = offset[owner[r]] + np.arange(grids[r].ntiles - 1)
+            for f in TILE_FIELDS:
+                srcs = [self._table_array(tab, f, dev) for tab in distinct]
+                arrays[f] = torch.cat([srcs[0][:1]] + [x[1:] for x in srcs])
+        else:
+            for f in TILE_FIELDS:
+                srcs = [self._table_array(tab, f, dev) for tab in tables]
+                a = torch.empty((nt,) + tuple(srcs[0].shape[1:]), dtype=srcs[0].dtype, device=dev)
+                a[0] = srcs[0][0]
+                for r, src in enumerate(srcs):
+                    a.index_copy_(0, torch.as_tensor(self.map[r][1:], device=dev), src[1:])
+                arrays[f] = a
         self.tables = DeviceGridTables(grid, rows, arrays)
+        self.table_tile = table_tile
         self.dx = np.array([g.dx for g in grids], np.float32)
         record = NumericsRecord.from_config(self.num, float(grids[0].dx))
-        self.backend = B200Backend(self.tables, record, device=dev, tile_run=tile_run, nruns=n)
+        self.backend = B200Backend(self.tables, record, device=dev, tile_run=tile_run, nruns=n, grid=grid,
+                                   table_tile=table_tile)  # fmt: skip
         for f in ("dtab", "ftabx", "ftaby"):  # packed into level-major pairs and quads by the backend
             del arrays[f]
         _lib.call("w2b_set_run_dx", self.backend.handle, self.dx.ctypes.data, n)

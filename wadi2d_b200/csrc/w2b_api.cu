@@ -169,6 +169,7 @@ static StepArgs make_args(const Handle& H) {
         A.ftab4[a] = reinterpret_cast<const float4*>(H.B.ftab4[a]);
     }
     A.dtab2 = reinterpret_cast<const float2*>(H.B.dtab2);
+    A.table_tile = H.B.table_tile;
     A.tiles = H.B.tiles;
     A.tile_of = H.B.tile_of;
     A.nbr = H.B.nbr;

@@ -110,6 +110,7 @@ struct StepArgs {
     const float* __restrict__ cw[2];
     const float2* __restrict__ dtab2;
     const float4* __restrict__ ftab4[2];
+    const int32_t* __restrict__ table_tile;  // the static and table tile of each tile, or null: its own
     const int32_t* __restrict__ tiles;
     const int32_t* __restrict__ tile_of;
     const int32_t* __restrict__ nbr;
@@ -357,6 +358,9 @@ __device__ __forceinline__ void face_lookup(float e, float top, const float4* __
     T = q.y + f * (q.w - q.y);
     W = qdiv(q.z - q.x, de);
 }
+
+// The tile whose static arrays and tables tile t reads (runs of a batch on one catchment share one copy).
+__device__ __forceinline__ int table_of(const StepArgs& A, int t) { return A.table_tile ? A.table_tile[t] : t; }
 
 // The tile holding NATIVE index k, and the tile-layout index of k's cell.
 __device__ __forceinline__ int tile_of_native(const StepArgs& A, int k) {

@@ -354,6 +354,7 @@ __global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_co
         const int want_wave = (flags & F_WAVE) != 0;
         const int p = A.R.parity[run];
         const int tj = A.tiles[2 * t], ti = A.tiles[2 * t + 1];
+        const int ts = table_of(A, t);
         if (tid == 0) {
             fence_proxy_async();
             mbar_expect_tx(&bar, (uint32_t)((NBOX - (want_wave ? 0 : 1)) * BOX + 14 * TILE2) * 4u);
@@ -369,7 +370,7 @@ __global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_co
             tma_load_2d(sm + F_ZCY * BOX, &M.zcy, x0, y0, &bar);
             tma_load_2d(sm + SM_M, &M.mx[p], x0 + 4, y0 + 2, &bar);
             tma_load_2d(sm + SM_M + TILE2, &M.my[p], x0 + 4, y0 + 2, &bar);
-            for (int f = 0; f < 12; ++f) bulk_load(sm + SM_ST + f * TILE2, statics[f] + (size_t)t * TILE2, TILE2 * 4, &bar);
+            for (int f = 0; f < 12; ++f) bulk_load(sm + SM_ST + f * TILE2, statics[f] + (size_t)ts * TILE2, TILE2 * 4, &bar);
         }
         const bool ok = mbar_wait(&bar, phase);
         phase ^= 1u;
@@ -388,10 +389,10 @@ __global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_co
             const int b = (jj + 2) * BOXW + ii + 4;
             const int k = base + jj * A.px + ii;
             FaceA fx, fy;
-            face_a<0>(sm, b, local, A, t, fx);
-            face_a<1>(sm, b, local, A, t, fy);
-            const float wx = face_bc<0>(sm, b, local, k, A, t, fx, dt, dx, want_wave, rowc, p);
-            const float wy = face_bc<1>(sm, b, local, k, A, t, fy, dt, dx, want_wave, rowc, p);
+            face_a<0>(sm, b, local, A, ts, fx);
+            face_a<1>(sm, b, local, A, ts, fy);
+            const float wx = face_bc<0>(sm, b, local, k, A, ts, fx, dt, dx, want_wave, rowc, p);
+            const float wy = face_bc<1>(sm, b, local, k, A, ts, fy, dt, dx, want_wave, rowc, p);
             wmax = fmax32(wmax, fmax32(wx, wy));
         }
         if (want_wave) {
@@ -432,7 +433,7 @@ __global__ void __launch_bounds__(1024) probe_kernel(StepArgs A, int t, float dt
         const size_t k = (size_t)(tj * TILE + GY + idx / TILE) * A.px + ti * TILE + GX + idx % TILE;
         sm[SM_M + idx] = A.mm[0][p][k];
         sm[SM_M + TILE2 + idx] = A.mm[1][p][k];
-        for (int f = 0; f < 12; ++f) sm[SM_ST + f * TILE2 + idx] = statics[f][(size_t)t * TILE2 + idx];
+        for (int f = 0; f < 12; ++f) sm[SM_ST + f * TILE2 + idx] = statics[f][(size_t)table_of(A, t) * TILE2 + idx];
     }
     if (tid < A.rows - 1) {
         const float m = (float)(A.rows - 1);
@@ -451,10 +452,11 @@ __global__ void __launch_bounds__(1024) probe_kernel(StepArgs A, int t, float dt
     const int b = (jj + 2) * BOXW + ii + 4;
     const int k = (tj * TILE + GY + jj) * A.px + ti * TILE + GX + ii;
     FaceA fx, fy;
-    face_a<0>(sm, b, local, A, t, fx);
-    face_a<1>(sm, b, local, A, t, fy);
-    out[local] = face_bc<0, true>(sm, b, local, k, A, t, fx, dt, dx, 1, rowc, p, out + 2 * TILE2);
-    out[TILE2 + local] = face_bc<1, true>(sm, b, local, k, A, t, fy, dt, dx, 1, rowc, p, out + 3 * TILE2);
+    const int ts = table_of(A, t);
+    face_a<0>(sm, b, local, A, ts, fx);
+    face_a<1>(sm, b, local, A, ts, fy);
+    out[local] = face_bc<0, true>(sm, b, local, k, A, ts, fx, dt, dx, 1, rowc, p, out + 2 * TILE2);
+    out[TILE2 + local] = face_bc<1, true>(sm, b, local, k, A, ts, fy, dt, dx, 1, rowc, p, out + 3 * TILE2);
 }
 
 void launch_probe(const StepArgs& A, int t, float dt, float* out, cudaStream_t s) {
@@ -510,7 +512,7 @@ __device__ __forceinline__ void update_issue(float* sm, uint64_t* bar, const TMa
     tma_load_2d(sm + U_H * BOX, &M.h[p], x0, y0, bar);
     tma_load_2d(sm + U_OWN, &M.res, x0 + 4, y0 + 2, bar);
     tma_load_2d(sm + U_OWN + TILE2, &M.src, x0 + 4, y0 + 2, bar);
-    bulk_load(sm + U_OWN + 2 * TILE2, A.hc + (size_t)t * TILE2, TILE2 * 4, bar);
+    bulk_load(sm + U_OWN + 2 * TILE2, A.hc + (size_t)table_of(A, t) * TILE2, TILE2 * 4, bar);
 }
 
 // The update pass (wadi2d/solver/gpu/kernels/cells.cu:4-63 with limit fused in): TMA stages the tile's unscaled
@@ -572,7 +574,7 @@ __global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_con
         }
         __syncthreads();
         const int base = (tj * TILE + GY) * px + ti * TILE + GX;
-        const float2* __restrict__ pairs_t = A.dtab2 + (size_t)t * (rows - 1) * TILE2;
+        const float2* __restrict__ pairs_t = A.dtab2 + (size_t)table_of(A, t) * (rows - 1) * TILE2;
         // continuity (cells.cu:219-232) for the thread's four cells
         float hn[4], sv[4], hcs[4];
         int rr[4];
@@ -1029,13 +1031,14 @@ __global__ void __launch_bounds__(256) plan_kernel(StepArgs A, const int32_t* li
         const int t = list[a];
         const int tj = A.tiles[2 * t], ti = A.tiles[2 * t + 1];
         const int base = (tj * TILE + GY) * A.px + ti * TILE + GX;
-        const float2* pairs_t = A.dtab2 + (size_t)t * (A.rows - 1) * TILE2;
+        const int ts = table_of(A, t);
+        const float2* pairs_t = A.dtab2 + (size_t)ts * (A.rows - 1) * TILE2;
         const float* h = A.hh[A.R.parity[A.tile_run[t]]];
         for (int c = 0; c < 4; ++c) {
             const int jj = threadIdx.y * 4 + c, ii = threadIdx.x;
             const int local = jj * TILE + ii;
             const int k = base + jj * A.px + ii;
-            A.om[k] = cell_plan(h[k], A.hc[t * TILE2 + local], pairs_t + local, A.rows);
+            A.om[k] = cell_plan(h[k], A.hc[ts * TILE2 + local], pairs_t + local, A.rows);
         }
     }
 }

@@ -151,6 +151,8 @@ class Model64(O.Model):
             refresh = self.refresh_due or self.nsteps % num.dt_every == 0
             self.refresh_due = False
             activate = self.nsteps % num.active_every == 0
+            if self.kick is not None:
+                self.kick.apply(b, float(dt))
             b.step(float(dt), refresh, activate)
             self.dts.append(float(dt))
             self.t += float(dt)

@@ -72,7 +72,9 @@ __device__ __forceinline__ FaceIn face_in(const float* sm, int b, int local) {
 }
 
 // Part A of the face of axis AX at box index b (wadi2d/solver/gpu/kernels/faces.cu:19-44).
-template <int AX>
+// ON: the numerics switches (second-order momentum, sheet flow, dry-face mirroring, depth carry) are all on, as the
+// reference's defaults have them, and known to the compiler; otherwise they are read from A.P.
+template <int AX, bool ON = false>
 __device__ __forceinline__ void face_a(const float* sm, int b, int local, const StepArgs& A, int t, FaceA& F) {
     constexpr int S = AX == 0 ? 1 : BOXW;
     const W2BParams& P = A.P;
@@ -85,7 +87,7 @@ __device__ __forceinline__ void face_a(const float* sm, int b, int local, const 
     const float cwf = st[5 * TILE2 + local];
     const float top = st[4 * TILE2 + local];
     float eface = eup;
-    if (P.carry && cwf == 0.0f) {
+    if ((ON || P.carry) && cwf == 0.0f) {
         const float* ZC = sm + (AX == 0 ? F_ZCX : F_ZCY) * BOX;
         const float dz = from_left ? ZC[b - S] - st[0 * TILE2 + local] : ZC[b] - st[1 * TILE2 + local];
         if (dz > 1e-6f) {
@@ -106,7 +108,7 @@ __device__ __forceinline__ void face_a(const float* sm, int b, int local, const 
 // Parts B and C: the momentum terms (faces.cu:50-100, table-free), then the lookup, section, friction, crest cap,
 // outputs and wave speed (faces.cu:43-44, :52-63, :102-145). Returns the wave speed.
 // PROBE: write the face's new velocity to probe_un[local] and nothing of the state (the step-limiter probe).
-template <int AX, bool PROBE = false>
+template <int AX, bool PROBE = false, bool ON = false>
 __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int k, const StepArgs& A, int t,
                                          const FaceA& F, float dt, float dx, int want_wave, const float* rowc, int p,
                                          float* probe_un = nullptr) {
@@ -140,7 +142,7 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
 
     // [1] section: the disconnected drive (the volume-limited section needs the table, below)
     float d_eta = I.e_rp - I.e_lp;
-    if (P.sheet) {
+    if (ON || P.sheet) {
         const float edown = from_left ? I.e_rp : I.e_lp;
         if (edown <= ZERO) {
             const float g_u = from_left ? st[2 * TILE2 + local] : st[3 * TILE2 + local];
@@ -153,7 +155,7 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
         }
     }
     // [3] momentum fluxes
-    const int mirror = P.mirror, second = P.second;
+    const int mirror = ON ? 1 : P.mirror, second = ON ? 1 : P.second;
     const float um = gated(U[b - S], uf, mirror);
     const float up = gated(U[b + S], uf, mirror);
     const float umm = gated(U[b - 2 * S], um, mirror);
@@ -227,7 +229,7 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
     }
     // [1] the volume-limited section
     float rho = ONE;
-    if (P.sheet) {
+    if (ON || P.sheet) {
         const float avol = hup * dx;
         if (avol < area) {
             const float sub = qdiv(fmin32(I.e_lp, I.e_rp), fmax32(I.e_lp, I.e_rp));
@@ -315,6 +317,7 @@ __device__ __forceinline__ float block_max(float v, float* red) {
 // 40 x 36 state boxes, the two momenta, and the tile's twelve static face scalars as bulk copies; on refresh steps
 // the tile's wave maximum goes to its run's maximum (an integer atomic max on the float bits). p is the parity of
 // the run's ping-pong halves.
+template <bool ON>
 __global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_constant__ TMaps M, StepArgs A) {
     extern __shared__ __align__(128) float sm[];
     __shared__ __align__(8) uint64_t bar;
@@ -389,10 +392,10 @@ __global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_co
             const int b = (jj + 2) * BOXW + ii + 4;
             const int k = base + jj * A.px + ii;
             FaceA fx, fy;
-            face_a<0>(sm, b, local, A, ts, fx);
-            face_a<1>(sm, b, local, A, ts, fy);
-            const float wx = face_bc<0>(sm, b, local, k, A, ts, fx, dt, dx, want_wave, rowc, p);
-            const float wy = face_bc<1>(sm, b, local, k, A, ts, fy, dt, dx, want_wave, rowc, p);
+            face_a<0, ON>(sm, b, local, A, ts, fx);
+            face_a<1, ON>(sm, b, local, A, ts, fy);
+            const float wx = face_bc<0, false, ON>(sm, b, local, k, A, ts, fx, dt, dx, want_wave, rowc, p);
+            const float wy = face_bc<1, false, ON>(sm, b, local, k, A, ts, fy, dt, dx, want_wave, rowc, p);
             wmax = fmax32(wmax, fmax32(wx, wy));
         }
         if (want_wave) {
@@ -464,19 +467,28 @@ void launch_probe(const StepArgs& A, int t, float dt, float* out, cudaStream_t s
 }
 
 cudaError_t faces_setup() {
-    const cudaError_t e = cudaFuncSetAttribute(probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SM_FLOATS * 4);
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(faces_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, FACES_SMEM);
+    cudaError_t e = cudaFuncSetAttribute(probe_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, SM_FLOATS * 4);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(faces_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    FACES_SMEM);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(faces_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                    FACES_SMEM);
+    return e;
 }
 
+// The resident CTAs a SM of the face pass (the smaller of its two forms').
 int faces_occupancy() {
-    int occ = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, faces_kernel, FACES_THREADS, FACES_SMEM);
-    return occ;
+    int on = 0, off = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&on, faces_kernel<true>, FACES_THREADS, FACES_SMEM);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&off, faces_kernel<false>, FACES_THREADS, FACES_SMEM);
+    return on < off ? on : off;
 }
 
+// The face pass, in its form with the numerics switches folded in when they are all on (the reference's defaults).
 void launch_faces(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s) {
-    faces_kernel<<<grid, FACES_THREADS, FACES_SMEM, s>>>(M, A);
+    if (A.P.second && A.P.sheet && A.P.mirror && A.P.carry)
+        faces_kernel<true><<<grid, FACES_THREADS, FACES_SMEM, s>>>(M, A);
+    else
+        faces_kernel<false><<<grid, FACES_THREADS, FACES_SMEM, s>>>(M, A);
 }
 
 // ------------------------------------------------------------------ update pass

@@ -56,9 +56,10 @@ def parse():
     p.add_argument("--steps", type=int, default=200)
     p.add_argument("--warmup", type=int, default=5)
     p.add_argument("--impl", default="b200", choices=("b200", "reference"))
-    p.add_argument("--arith", default="exact", choices=("exact", "fast"),
-                   help="the step's build: exact (the reference's float32 bits) or fast (FMA contraction, approximate "
-                        "division, square root and cube root in the face pass)")
+    p.add_argument("--arith", default="fast", choices=("exact", "fast"),
+                   help="the step's build: fast (the default: FMA contraction, approximate division, square root and "
+                        "powers in the face pass, held to the step's accuracy bounds against the oracle and the FP64 "
+                        "run) or exact (the reference's float32 bits)")
     p.add_argument("--parity-steps", type=int, default=200,
                    help="steps of the CUDA path against the oracle on the CPU sample block (0: none)")
     p.add_argument("--n", type=int, default=4096, help="domain side in cells (configuration 3: 4096)")

@@ -365,14 +365,18 @@ class B200Backend:
         """The device loop's launch schedule (w2b_loop_config): the face and update passes' CTAs a SM and the loop
         steps a captured graph (while the tuner runs: the next graph launch's), whether it is still tuning, and each
         pass's resident CTAs a SM."""
-        out = np.zeros(6, np.int32)
+        out = np.zeros(8, np.int32)
         _lib.call("w2b_loop_config", self.handle, out.ctypes.data)
-        keys = ("faces_per_sm", "update_per_sm", "steps_per_graph", "tuning", "faces_occupancy", "update_occupancy")
+        keys = ("faces_per_sm", "update_per_sm", "steps_per_graph", "tuning", "faces_occupancy", "update_occupancy",
+                "strips", "strips_occupancy")  # fmt: skip
         return {k: int(v) for k, v in zip(keys, out, strict=True)}
 
-    def set_loop(self, tune: bool = True, faces_per_sm: int = 0, update_per_sm: int = 0, steps: int = 0) -> None:
-        """Start the launch tuner again (``tune``), or fix the device loop's launch schedule (w2b_loop_tuning)."""
-        _lib.call("w2b_loop_tuning", self.handle, int(bool(tune)), int(faces_per_sm), int(update_per_sm), int(steps))
+    def set_loop(self, tune: bool = True, faces_per_sm: int = 0, update_per_sm: int = 0, steps: int = 0,
+                 strips: bool = False) -> None:  # fmt: skip
+        """Start the launch tuner again (``tune``), or fix the device loop's launch schedule (w2b_loop_tuning): the face
+        pass's CTAs a SM in its tile form, or with ``strips`` in its strip form, the update pass's, steps a graph."""
+        code = 1 if tune else (2 if strips else 0)
+        _lib.call("w2b_loop_tuning", self.handle, code, int(faces_per_sm), int(update_per_sm), int(steps))
 
     def max_wave(self) -> float:
         w = ctypes.c_float()

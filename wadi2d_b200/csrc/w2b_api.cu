@@ -22,7 +22,9 @@ namespace w2b {
     void launch_faces(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s); \
     cudaError_t update_setup();                                                     \
     int update_occupancy();                                                         \
-    void launch_update(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s);
+    void launch_update(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s); \
+    int strips_occupancy();                                                         \
+    void launch_strips(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s);
 namespace exact {
 W2B_PASSES_DECL
 }
@@ -39,13 +41,15 @@ struct Passes {
     cudaError_t (*update_setup)();
     int (*update_occupancy)();
     void (*launch_update)(const TMaps&, const StepArgs&, int, cudaStream_t);
+    int (*strips_occupancy)();
+    void (*launch_strips)(const TMaps&, const StepArgs&, int, cudaStream_t);
 };
 static const Passes EXACT_PASSES = {exact::faces_setup,  exact::launch_probe,     exact::faces_occupancy,
                                     exact::launch_faces, exact::update_setup,     exact::update_occupancy,
-                                    exact::launch_update};
+                                    exact::launch_update, exact::strips_occupancy, exact::launch_strips};
 static const Passes FAST_PASSES = {fast::faces_setup,  fast::launch_probe,     fast::faces_occupancy,
                                    fast::launch_faces, fast::update_setup,     fast::update_occupancy,
-                                   fast::launch_update};
+                                   fast::launch_update,  fast::strips_occupancy,  fast::launch_strips};
 static const Passes& passes(const W2BParams& P) { return P.arith == W2B_ARITH_FAST ? FAST_PASSES : EXACT_PASSES; }
 
 void launch_cbrt_check(uint32_t first, uint32_t count, unsigned long long* out, cudaStream_t s);
@@ -67,13 +71,15 @@ __global__ void pack_tables_kernel(const float* dtab, const float* ftabx, const 
                                    float4* fx, float4* fy, int ntiles, int rows);
 __global__ void bmark_kernel(StepArgs A, int clear_words);
 
-// A launch configuration of the device loop: CTAs a SM of the face pass and of the update pass, and loop steps a
-// captured graph. Every configuration computes the same bits (a tile's arithmetic does not depend on the grid, and
-// the wave maximum is an order-free integer max); they differ only in time.
+// A launch configuration of the device loop: the face pass's form (whole tiles, or the strip form: half tiles in
+// smaller CTAs), its CTAs a SM, the update pass's CTAs a SM, and loop steps a captured graph. Every configuration
+// computes the same bits (a face's arithmetic does not depend on the form or the grid, and the wave maximum is an
+// order-free integer max); they differ only in time.
 struct LoopConfig {
     int faces_per_sm, update_per_sm, steps;
+    int strips;
 };
-constexpr int TUNE_CANDIDATES = 5;               // the default and one change of each knob either way
+constexpr int TUNE_CANDIDATES = 6;               // the default, one change of each knob either way, the strip form
 constexpr int FORCED = TUNE_CANDIDATES;          // the slot of a configuration the caller fixes
 constexpr int TUNE_SAMPLES = 3;                  // timed graph launches a candidate before the tuner settles
 constexpr int MAX_GRAPH_STEPS = 64;
@@ -125,6 +131,7 @@ struct Handle {
     int step_blocks = 148;   // resident CTAs of the update pass
     int faces_blocks = 296;  // resident CTAs of the face pass
     int faces_occ = 2, update_occ = 1;  // resident CTAs a SM of the two passes
+    int strips_occ = 4;                 // resident CTAs a SM of the face pass's strip form
     TMaps tmaps;
     unsigned version = 0;   // bumped whenever a graph would capture stale arguments
     Loop loop;
@@ -287,6 +294,25 @@ static int build_tmaps(Handle& H) {
         own(&H.tmaps.mx[p], B.mx[p]);
         own(&H.tmaps.my[p], B.my[p]);
     }
+    // the strip form's boxes: 40 x 20 (half a tile and its halo), 32 x 16 for the momenta
+    auto strip = [&](CUtensorMap* m, const float* q) {
+        if (st == W2B_OK) st = encode_2d(enc, m, q, H.g, H.L, 40, 20);
+    };
+    auto strip_own = [&](CUtensorMap* m, const float* q) {
+        if (st == W2B_OK) st = encode_2d(enc, m, q, H.g, H.L, 32, 16);
+    };
+    strip(&H.tmaps.sd, B.d);
+    strip(&H.tmaps.sqx, B.qx);
+    strip(&H.tmaps.sqy, B.qy);
+    strip(&H.tmaps.szcx, B.zcx);
+    strip(&H.tmaps.szcy, B.zcy);
+    for (int p = 0; p < 2; ++p) {
+        strip(&H.tmaps.sh[p], B.h[p]);
+        strip(&H.tmaps.su[p], B.u[p]);
+        strip(&H.tmaps.sv[p], B.v[p]);
+        strip_own(&H.tmaps.smx[p], B.mx[p]);
+        strip_own(&H.tmaps.smy[p], B.my[p]);
+    }
     return st;
 }
 
@@ -303,16 +329,18 @@ static void drop_graphs(Handle& H) {
 }
 
 // The tuner's candidates: the occupancy-given default (both passes at their resident CTAs a SM, 16 steps a graph),
-// and from it one CTA a SM fewer in the face pass, half the update pass's, 8 and 32 steps a graph.
+// and from it one CTA a SM fewer in the face pass, half the update pass's, 8 and 32 steps a graph, and the face pass
+// in its strip form at its resident CTAs a SM.
 static void init_loop(Handle& H) {
     Loop& L = H.loop;
     const int F = H.faces_occ, U = H.update_occ;
     L.ncand = 0;
-    L.cand[L.ncand++] = {F, U, 16};
-    if (F > 1) L.cand[L.ncand++] = {F - 1, U, 16};
-    if (U > 1) L.cand[L.ncand++] = {F, (U + 1) / 2, 16};
-    L.cand[L.ncand++] = {F, U, 8};
-    L.cand[L.ncand++] = {F, U, 32};
+    L.cand[L.ncand++] = {F, U, 16, 0};
+    if (F > 1) L.cand[L.ncand++] = {F - 1, U, 16, 0};
+    if (U > 1) L.cand[L.ncand++] = {F, (U + 1) / 2, 16, 0};
+    L.cand[L.ncand++] = {F, U, 8, 0};
+    L.cand[L.ncand++] = {F, U, 32, 0};
+    L.cand[L.ncand++] = {H.strips_occ, U, 16, 1};
     L.cand[FORCED] = L.cand[0];
     for (int c = 0; c < TUNE_CANDIDATES; ++c) {
         L.sec[c] = 0.0;
@@ -344,13 +372,26 @@ static int set_passes(Handle& H) {
             return cuda_status(cudaGetLastError(), "pass setup");
     }
     const Passes& X = passes(H.P);
-    const int occ = X.update_occupancy(), focc = X.faces_occupancy();
+    const int occ = X.update_occupancy(), focc = X.faces_occupancy(), socc = X.strips_occupancy();
     H.update_occ = occ > 0 ? occ : 1;
     H.faces_occ = focc > 0 ? focc : 1;
+    H.strips_occ = socc > 0 ? socc : 1;
     H.step_blocks = H.sms * H.update_occ;
     H.faces_blocks = H.sms * H.faces_occ;
     init_loop(H);
     return W2B_OK;
+}
+
+// The face pass of a host-driven step (w2b_step, w2b_step_timed) over n tiles: in the form and at the CTAs a SM the
+// device loop's tuner settled on, the tile form while it tunes.
+static void launch_faces_host(Handle& H, const StepArgs& A, int n, cudaStream_t s) {
+    const LoopConfig& C = H.loop.cand[H.loop.chosen];
+    if (!H.loop.tuning && C.strips) {
+        const int g = H.sms * C.faces_per_sm;
+        passes(H.P).launch_strips(H.tmaps, A, 2 * n < g ? 2 * n : g, s);
+    } else {
+        passes(H.P).launch_faces(H.tmaps, A, faces_grid(H, n), s);
+    }
 }
 
 // One step of the device loop under launch configuration C: every running run advances by one of its own steps.
@@ -362,7 +403,10 @@ static int launch_loop_step(Handle& H, const LoopConfig& C, cudaStream_t s) {
     const int tiles = H.g.ntiles - 1 > 0 ? H.g.ntiles - 1 : 1;
     const int fgrid = H.sms * C.faces_per_sm, ugrid = H.sms * C.update_per_sm;
     const Passes& X = passes(H.P);
-    X.launch_faces(H.tmaps, A, tiles < fgrid ? tiles : fgrid, s);
+    if (C.strips)
+        X.launch_strips(H.tmaps, A, 2 * tiles < fgrid ? 2 * tiles : fgrid, s);
+    else
+        X.launch_faces(H.tmaps, A, tiles < fgrid ? tiles : fgrid, s);
     X.launch_update(H.tmaps, A, tiles < ugrid ? tiles : ugrid, s);
     envelope_kernel<<<H.sms * 2, TILE2, 0, s>>>(A);
     boundary_kernel<<<boundary_grid(H, 1), 256, 0, s>>>(A, 1);
@@ -597,7 +641,7 @@ int32_t w2b_step(void* handle, float dt, int32_t want_wave, int32_t want_wet, vo
         return W2B_OK;
     }
     const int grid = blocks_for(*H, H->nact);
-    passes(H->P).launch_faces(H->tmaps, A, faces_grid(*H, H->nact), s);
+    launch_faces_host(*H, A, H->nact, s);
     passes(H->P).launch_update(H->tmaps, A, grid, s);
     if (H->nb) boundary_kernel<<<boundary_grid(*H, 0), 256, 0, s>>>(A, 0);
     endstep_kernel<<<1, 1, 0, s>>>(A);
@@ -618,7 +662,7 @@ int32_t w2b_step_timed(void* handle, float dt, int32_t want_wave, int32_t want_w
     setstep_kernel<<<1, 1, 0, s>>>(A, dt, want_wave, want_wet, H->nact);
     const int grid = blocks_for(*H, H->nact);
     CK(cudaEventRecord(ev[0], s));
-    passes(H->P).launch_faces(H->tmaps, A, faces_grid(*H, H->nact), s);
+    launch_faces_host(*H, A, H->nact, s);
     CK(cudaEventRecord(ev[1], s));
     passes(H->P).launch_update(H->tmaps, A, grid, s);
     CK(cudaEventRecord(ev[2], s));
@@ -946,15 +990,17 @@ int32_t w2b_loop_tuning(void* handle, int32_t tune, int32_t faces_per_sm, int32_
     if (!handle) return W2B_EINVAL;
     Handle* H = static_cast<Handle*>(handle);
     Loop& L = H->loop;
-    if (tune) {
+    if (tune == 1) {
         drop_graphs(*H);
         init_loop(*H);
         return W2B_OK;
     }
-    if (faces_per_sm < 1 || faces_per_sm > H->faces_occ || update_per_sm < 1 || update_per_sm > H->update_occ ||
-        steps < 1 || steps > MAX_GRAPH_STEPS)
+    const int strips = tune == 2;
+    if (tune != 0 && tune != 2) return W2B_EINVAL;
+    if (faces_per_sm < 1 || faces_per_sm > (strips ? H->strips_occ : H->faces_occ) || update_per_sm < 1 ||
+        update_per_sm > H->update_occ || steps < 1 || steps > MAX_GRAPH_STEPS)
         return W2B_EINVAL;
-    L.cand[FORCED] = {faces_per_sm, update_per_sm, steps};
+    L.cand[FORCED] = {faces_per_sm, update_per_sm, steps, strips};
     drop_graph(*H, FORCED);
     L.chosen = FORCED;
     L.tuning = 0;
@@ -972,6 +1018,8 @@ int32_t w2b_loop_config(void* handle, int32_t* out) {
     out[3] = L.tuning;
     out[4] = H->faces_occ;
     out[5] = H->update_occ;
+    out[6] = C.strips;
+    out[7] = H->strips_occ;
     return W2B_OK;
 }
 

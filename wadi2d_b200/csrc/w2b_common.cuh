@@ -161,6 +161,8 @@ struct TMaps {
     CUtensorMap d, h[2], u[2], v[2], qx, qy, om, zcx, zcy, mx[2], my[2];
     CUtensorMap qx1, qy1;  // 40 x 36 boxes for the update pass
     CUtensorMap res, src;  // 32 x 32 boxes
+    // the strip form of the face pass (half a tile, 16 rows): 40 x 20 boxes, and 32 x 16 for the momenta
+    CUtensorMap sd, sh[2], su[2], sv[2], sqx, sqy, szcx, szcy, smx[2], smy[2];
 };
 
 // ------------------------------------------------------------------ float32 helpers

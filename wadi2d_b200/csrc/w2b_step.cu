@@ -40,6 +40,23 @@ constexpr int SM_FLOATS = SM_ST + 12 * TILE2;
 constexpr int FACES_SMEM = SM_FLOATS * 4;  // 109,184 bytes: two CTAs a SM
 constexpr int FACES_THREADS = 512;
 
+// The two images the face helpers read. A whole tile (the face pass and the probe): nine 40 x 36 boxes, the plan
+// share among them. A strip (half a tile, 16 rows: the strip form of the face pass): eight 40 x 20 boxes, the plan
+// share read from global memory on the refresh steps that want it. S is the stride of a static face scalar's (and of
+// a momentum's) array in the image: 1,024 floats for a tile, 512 for a strip.
+struct TileImage {
+    static constexpr int BOX = w2b::W2B_ARITH::BOX, ZCX = F_ZCX, ZCY = F_ZCY, M = SM_M, ST = SM_ST, S = TILE2;
+    static constexpr bool OM = true;
+};
+constexpr int SROWS = 16, SBOXH = SROWS + 4, SBOX = BOXW * SBOXH, SNBOX = 8, STILE = TILE * SROWS;
+struct StripImage {
+    static constexpr int BOX = SBOX, ZCX = 6, ZCY = 7, M = SNBOX * SBOX, ST = SNBOX * SBOX + 2 * STILE, S = STILE;
+    static constexpr bool OM = false;
+};
+constexpr int STRIP_FLOATS = StripImage::ST + 12 * STILE;
+constexpr int STRIP_SMEM = STRIP_FLOATS * 4;  // 54,272 bytes: four CTAs a SM
+constexpr int STRIP_THREADS = 256;
+
 // What the first part of a face hands to the rest: the row's quad (its load is issued in part A and consumed after
 // the table-free momentum terms), the face depth, and the table row with the upwind choice, the live flag and the
 // above-the-table flag packed in one word. Parts B and C re-read the other inputs from the tile's image, so few
@@ -56,15 +73,15 @@ constexpr int FA_ROW = 0xff, FA_LEFT = 0x100, FA_LIVE = 0x200, FA_ABOVE = 0x400;
 struct FaceIn {
     float e_l, e_r, e_lp, e_rp, uf;
 };
-template <int AX>
-__device__ __forceinline__ FaceIn face_in(const float* sm, int b, int local) {
+template <int AX, class L>
+__device__ __forceinline__ FaceIn face_in(const float* sm, int b, int sl) {
     constexpr int S = AX == 0 ? 1 : BOXW;
-    const float* D = sm + F_D * BOX;
-    const float* U = sm + (AX == 0 ? F_U : F_V) * BOX;
-    const float* st = sm + SM_ST + AX * 6 * TILE2;
+    const float* D = sm + F_D * L::BOX;
+    const float* U = sm + (AX == 0 ? F_U : F_V) * L::BOX;
+    const float* st = sm + L::ST + AX * 6 * L::S;
     FaceIn I;
-    I.e_l = D[b - S] - st[0 * TILE2 + local];
-    I.e_r = D[b] - st[1 * TILE2 + local];
+    I.e_l = D[b - S] - st[0 * L::S + sl];
+    I.e_r = D[b] - st[1 * L::S + sl];
     I.uf = U[b];
     I.e_lp = fmax32(I.e_l, 0.0f);
     I.e_rp = fmax32(I.e_r, 0.0f);
@@ -74,22 +91,24 @@ __device__ __forceinline__ FaceIn face_in(const float* sm, int b, int local) {
 // Part A of the face of axis AX at box index b (wadi2d/solver/gpu/kernels/faces.cu:19-44).
 // ON: the numerics switches (second-order momentum, sheet flow, dry-face mirroring, depth carry) are all on, as the
 // reference's defaults have them, and known to the compiler; otherwise they are read from A.P.
-template <int AX, bool ON = false>
-__device__ __forceinline__ void face_a(const float* sm, int b, int local, const StepArgs& A, int t, FaceA& F) {
+// L: the image (TileImage, StripImage); sl: the cell's index in the image's static arrays, local: in the tile.
+template <int AX, bool ON = false, class L = TileImage>
+__device__ __forceinline__ void face_a(const float* sm, int b, int sl, int local, const StepArgs& A, int t,
+                                       FaceA& F) {
     constexpr int S = AX == 0 ? 1 : BOXW;
     const W2BParams& P = A.P;
-    const float* st = sm + SM_ST + AX * 6 * TILE2;
-    const FaceIn I = face_in<AX>(sm, b, local);
+    const float* st = sm + L::ST + AX * 6 * L::S;
+    const FaceIn I = face_in<AX, L>(sm, b, sl);
     const bool from_left = I.uf > 0.0f || (I.uf == 0.0f && I.e_l >= I.e_r);
     const float eup = from_left ? I.e_lp : I.e_rp;
     F.bits = from_left ? FA_LEFT : 0;
     if (eup <= P.e_wet) return;
-    const float cwf = st[5 * TILE2 + local];
-    const float top = st[4 * TILE2 + local];
+    const float cwf = st[5 * L::S + sl];
+    const float top = st[4 * L::S + sl];
     float eface = eup;
     if ((ON || P.carry) && cwf == 0.0f) {
-        const float* ZC = sm + (AX == 0 ? F_ZCX : F_ZCY) * BOX;
-        const float dz = from_left ? ZC[b - S] - st[0 * TILE2 + local] : ZC[b] - st[1 * TILE2 + local];
+        const float* ZC = sm + (AX == 0 ? L::ZCX : L::ZCY) * L::BOX;
+        const float dz = from_left ? ZC[b - S] - st[0 * L::S + sl] : ZC[b] - st[1 * L::S + sl];
         if (dz > 1e-6f) {
             float phi = qdiv(eup - 2.0f * dz, 2.0f * dz);
             phi = phi < 0.0f ? 0.0f : (phi > 1.0f ? 1.0f : phi);
@@ -108,8 +127,8 @@ __device__ __forceinline__ void face_a(const float* sm, int b, int local, const 
 // Parts B and C: the momentum terms (faces.cu:50-100, table-free), then the lookup, section, friction, crest cap,
 // outputs and wave speed (faces.cu:43-44, :52-63, :102-145). Returns the wave speed.
 // PROBE: write the face's new velocity to probe_un[local] and nothing of the state (the step-limiter probe).
-template <int AX, bool PROBE = false, bool ON = false>
-__device__ __forceinline__ float face_bc(const float* sm, int b, int local, int k, const StepArgs& A, int t,
+template <int AX, bool PROBE = false, bool ON = false, class L = TileImage>
+__device__ __forceinline__ float face_bc(const float* sm, int b, int sl, int local, int k, const StepArgs& A, int t,
                                          const FaceA& F, float dt, float dx, int want_wave, const float* rowc, int p,
                                          float* probe_un = nullptr) {
     constexpr int S = AX == 0 ? 1 : BOXW;
@@ -127,13 +146,13 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
     }
     const float ZERO = 0.0f, HALF = 0.5f, ONE = 1.0f;
     const float span = dx;
-    const float* H = sm + F_H * BOX;
-    const float* U = sm + (AX == 0 ? F_U : F_V) * BOX;
-    const float* VP = sm + (AX == 0 ? F_V : F_U) * BOX;
-    const float* Q = sm + (AX == 0 ? F_QX : F_QY) * BOX;
-    const float* QP = sm + (AX == 0 ? F_QY : F_QX) * BOX;
-    const float* st = sm + SM_ST + AX * 6 * TILE2;
-    const FaceIn I = face_in<AX>(sm, b, local);
+    const float* H = sm + F_H * L::BOX;
+    const float* U = sm + (AX == 0 ? F_U : F_V) * L::BOX;
+    const float* VP = sm + (AX == 0 ? F_V : F_U) * L::BOX;
+    const float* Q = sm + (AX == 0 ? F_QX : F_QY) * L::BOX;
+    const float* QP = sm + (AX == 0 ? F_QY : F_QX) * L::BOX;
+    const float* st = sm + L::ST + AX * 6 * L::S;
+    const FaceIn I = face_in<AX, L>(sm, b, sl);
     const bool from_left = (F.bits & FA_LEFT) != 0;
     const float uf = I.uf;
     const float eup = from_left ? I.e_lp : I.e_rp;
@@ -145,8 +164,8 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
     if (ON || P.sheet) {
         const float edown = from_left ? I.e_rp : I.e_lp;
         if (edown <= ZERO) {
-            const float g_u = from_left ? st[2 * TILE2 + local] : st[3 * TILE2 + local];
-            const float g_d = from_left ? st[3 * TILE2 + local] : st[2 * TILE2 + local];
+            const float g_u = from_left ? st[2 * L::S + sl] : st[3 * L::S + sl];
+            const float g_d = from_left ? st[3 * L::S + sl] : st[2 * L::S + sl];
             const float h_d = from_left ? h_r : h_l;
             const float drop = (hup - g_u) - fmax32(h_d - g_d, HALF * (g_u - g_d));
             const float level_drop = fabsf(I.e_l - I.e_r);
@@ -186,14 +205,14 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
     const float press = dt * P.g * d_eta * rspan;
     float us;
     if (abar > 1e-6f * dx)
-        us = qdiv(sm[SM_M + AX * TILE2 + local] - dt * flux * rspan, abar) - press;
+        us = qdiv(sm[L::M + AX * L::S + sl] - dt * flux * rspan, abar) - press;
     else
         us = uf - press;
 #else
     const float press = qdiv(dt * P.g * d_eta, span);
     float us;
     if (abar > 1e-6f * dx)
-        us = qdiv(sm[SM_M + AX * TILE2 + local] - qdiv(dt * flux, span), abar) - press;
+        us = qdiv(sm[L::M + AX * L::S + sl] - qdiv(dt * flux, span), abar) - press;
     else
         us = uf - press;
 #endif
@@ -202,7 +221,7 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
     // the table lookup from the quad loaded in part A (common.cuh face_lookup); rowc holds, per row r, c0^2 and
     // c1^2 - c0^2 with c0 = r / m, c1 = (r + 1) / m, and in its last slot 1 - c^2 with c = (m - 1) / m: the very
     // float32 values the lookup forms, computed once a CTA
-    const float top = st[4 * TILE2 + local], e = F.eface;
+    const float top = st[4 * L::S + sl], e = F.eface;
     const float4 q = F.q;
     float area, tt, w;
     if (F.bits & FA_ABOVE) {
@@ -254,7 +273,7 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
     if (fabsf(un) > P.u_max) un = un > ZERO ? P.u_max : -P.u_max;
     // [6] crest face
     float qn = area * rho * un;
-    float c = st[5 * TILE2 + local];
+    float c = st[5 * L::S + sl];
     if (c != ZERO) {
         float area_c = area, w_c = w;
         if (c < ZERO) {
@@ -279,14 +298,23 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int local, int 
     }
     if (!want_wave) return ZERO;
     if (not_finite(un)) return 1e30f;
-    const float* D = sm + F_D * BOX;
-    const float* OM = sm + F_OM * BOX;
+    const float* D = sm + F_D * L::BOX;
     const float d_left = D[b - S], d_right = D[b];
     const float dup = from_left ? d_left : d_right;
     if (dup <= P.h_cfl) return ZERO;
-    float plan = from_left ? OM[b - S] : OM[b];
+    // the plan shares of the face's two cells: from the image, or (a strip) from global memory at native index k
+    float om_l, om_r;
+    if constexpr (L::OM) {
+        const float* OM = sm + F_OM * L::BOX;
+        om_l = OM[b - S];
+        om_r = OM[b];
+    } else {
+        om_l = A.om[k - (AX == 0 ? 1 : A.px)];
+        om_r = A.om[k];
+    }
+    float plan = from_left ? om_l : om_r;
     const float dother = from_left ? d_right : d_left;
-    if (dother > P.h_cfl) plan = fmin32(plan, from_left ? OM[b] : OM[b - S]);
+    if (dother > P.h_cfl) plan = fmin32(plan, from_left ? om_r : om_l);
     const float wave = qsqrt(fmax32(qdiv(P.g * area * rho, fmax32(plan, P.a_min) * dx), ZERO));
     return fabsf(un) + fmin32(P.lead * fabsf(un - uf), 2.0f * wave) + wave;
 }
@@ -392,10 +420,10 @@ __global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_co
             const int b = (jj + 2) * BOXW + ii + 4;
             const int k = base + jj * A.px + ii;
             FaceA fx, fy;
-            face_a<0, ON>(sm, b, local, A, ts, fx);
-            face_a<1, ON>(sm, b, local, A, ts, fy);
-            const float wx = face_bc<0, false, ON>(sm, b, local, k, A, ts, fx, dt, dx, want_wave, rowc, p);
-            const float wy = face_bc<1, false, ON>(sm, b, local, k, A, ts, fy, dt, dx, want_wave, rowc, p);
+            face_a<0, ON>(sm, b, local, local, A, ts, fx);
+            face_a<1, ON>(sm, b, local, local, A, ts, fy);
+            const float wx = face_bc<0, false, ON>(sm, b, local, local, k, A, ts, fx, dt, dx, want_wave, rowc, p);
+            const float wy = face_bc<1, false, ON>(sm, b, local, local, k, A, ts, fy, dt, dx, want_wave, rowc, p);
             wmax = fmax32(wmax, fmax32(wx, wy));
         }
         if (want_wave) {
@@ -456,14 +484,119 @@ __global__ void __launch_bounds__(1024) probe_kernel(StepArgs A, int t, float dt
     const int k = (tj * TILE + GY + jj) * A.px + ti * TILE + GX + ii;
     FaceA fx, fy;
     const int ts = table_of(A, t);
-    face_a<0>(sm, b, local, A, ts, fx);
-    face_a<1>(sm, b, local, A, ts, fy);
-    out[local] = face_bc<0, true>(sm, b, local, k, A, ts, fx, dt, dx, 1, rowc, p, out + 2 * TILE2);
-    out[TILE2 + local] = face_bc<1, true>(sm, b, local, k, A, ts, fy, dt, dx, 1, rowc, p, out + 3 * TILE2);
+    face_a<0>(sm, b, local, local, A, ts, fx);
+    face_a<1>(sm, b, local, local, A, ts, fy);
+    out[local] = face_bc<0, true>(sm, b, local, local, k, A, ts, fx, dt, dx, 1, rowc, p, out + 2 * TILE2);
+    out[TILE2 + local] = face_bc<1, true>(sm, b, local, local, k, A, ts, fy, dt, dx, 1, rowc, p, out + 3 * TILE2);
 }
 
 void launch_probe(const StepArgs& A, int t, float dt, float* out, cudaStream_t s) {
     probe_kernel<<<1, 1024, SM_FLOATS * 4, s>>>(A, t, dt, out);
+}
+
+// The strip form of the face pass: the same faces, half a tile at a time. A unit of work is one 16-row half of a tile of
+// the work list (2 nwork units); a CTA of 256 threads (8 warps, a warp a strip row, two rows a warp) stages the strip
+// with TMA as eight 40 x 20 boxes, its momenta as 32 x 16 boxes and its twelve static face scalars as 2 KB bulk copies,
+// 54 KB in all, so that four CTAs share a SM and one waits for its copies while three compute (the tile form's two
+// CTAs of 109 KB leave a SM idle whenever both wait). The plan shares, wanted on refresh steps only, are read from
+// global memory. A face's arithmetic is the tile form's, bit for bit. On refresh steps each strip's wave maximum goes
+// to its tile's entry and its run's maximum by integer atomic maxima on the float bits.
+template <bool ON>
+__global__ void __launch_bounds__(STRIP_THREADS, 4) strips_kernel(const __grid_constant__ TMaps M, StepArgs A) {
+    extern __shared__ __align__(128) float sm[];
+    __shared__ __align__(8) uint64_t bar;
+    __shared__ float red[32];
+    __shared__ float rowc[2 * 64 + 1];
+    Ctl* ctl = A.ctl;
+    if (!(ctl->any & ANY_RUN)) return;
+    const int nunits = 2 * ctl->nwork;
+    const int tid = threadIdx.x;
+    if (tid == 0) {
+        mbar_init(&bar, 1);
+        fence_barrier_init();
+    }
+    if (tid < A.rows - 1) {
+        const float m = (float)(A.rows - 1);
+        const float c0 = (float)tid / m;
+        const float c1 = (float)(tid + 1) / m;
+        rowc[2 * tid] = c0 * c0;
+        rowc[2 * tid + 1] = c1 * c1 - c0 * c0;
+    } else if (tid == A.rows - 1) {
+        const float m = (float)(A.rows - 1);
+        const float c = (m - 1.0f) / m;
+        rowc[2 * tid] = 1.0f - c * c;
+    }
+    __syncthreads();
+    const float* statics[12] = {A.fl[0], A.fr[0], A.gl[0], A.gr[0], A.ef[0], A.cw[0],
+                                A.fl[1], A.fr[1], A.gl[1], A.gr[1], A.ef[1], A.cw[1]};
+    uint32_t phase = 0;
+    const int lane = tid & 31, warp = tid >> 5;
+    for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
+        const int t = A.list[u >> 1];
+        const int row0 = (u & 1) * SROWS;
+        const int run = A.tile_run[t];
+        const int flags = A.R.flags[run];
+        if (!(flags & F_RUN)) continue;  // the tile's run has finished: uniform over the CTA
+        const float dt = A.R.dtf[run];
+        const float dx = A.R.dx[run];
+        const int want_wave = (flags & F_WAVE) != 0;
+        const int p = A.R.parity[run];
+        const int tj = A.tiles[2 * t], ti = A.tiles[2 * t + 1];
+        const int ts = table_of(A, t);
+        if (tid == 0) {
+            fence_proxy_async();
+            mbar_expect_tx(&bar, (uint32_t)STRIP_SMEM);
+            const int x0 = ti * TILE + GX - 4, y0 = tj * TILE + GY + row0 - 2;
+            tma_load_2d(sm + F_D * SBOX, &M.sd, x0, y0, &bar);
+            tma_load_2d(sm + F_H * SBOX, &M.sh[p], x0, y0, &bar);
+            tma_load_2d(sm + F_U * SBOX, &M.su[p], x0, y0, &bar);
+            tma_load_2d(sm + F_V * SBOX, &M.sv[p], x0, y0, &bar);
+            tma_load_2d(sm + F_QX * SBOX, &M.sqx, x0, y0, &bar);
+            tma_load_2d(sm + F_QY * SBOX, &M.sqy, x0, y0, &bar);
+            tma_load_2d(sm + StripImage::ZCX * SBOX, &M.szcx, x0, y0, &bar);
+            tma_load_2d(sm + StripImage::ZCY * SBOX, &M.szcy, x0, y0, &bar);
+            tma_load_2d(sm + StripImage::M, &M.smx[p], x0 + 4, y0 + 2, &bar);
+            tma_load_2d(sm + StripImage::M + STILE, &M.smy[p], x0 + 4, y0 + 2, &bar);
+            for (int f = 0; f < 12; ++f)
+                bulk_load(sm + StripImage::ST + f * STILE, statics[f] + (size_t)ts * TILE2 + row0 * TILE, STILE * 4,
+                          &bar);
+        }
+        const bool ok = mbar_wait(&bar, phase);
+        phase ^= 1u;
+        if (__syncthreads_or(!ok)) {
+            // the copies did not land: report, give them one more bounded wait, and leave the loop
+            if (tid == 0) atomicExch(&ctl->status, W2B_ETIMEOUT);
+            mbar_wait(&bar, phase ^ 1u);
+            return;
+        }
+        const int base = (tj * TILE + GY) * A.px + ti * TILE + GX;
+        float wmax = 0.0f;
+#pragma unroll 1
+        for (int c = 0; c < 2; ++c) {
+            const int js = warp + 8 * c, ii = lane;  // the row in the strip, and in the tile
+            const int jj = row0 + js;
+            const int sl = js * TILE + ii, local = jj * TILE + ii;
+            const int b = (js + 2) * BOXW + ii + 4;
+            const int k = base + jj * A.px + ii;
+            FaceA fx, fy;
+            face_a<0, ON, StripImage>(sm, b, sl, local, A, ts, fx);
+            face_a<1, ON, StripImage>(sm, b, sl, local, A, ts, fy);
+            const float wx = face_bc<0, false, ON, StripImage>(sm, b, sl, local, k, A, ts, fx, dt, dx, want_wave, rowc,
+                                                               p);
+            const float wy = face_bc<1, false, ON, StripImage>(sm, b, sl, local, k, A, ts, fy, dt, dx, want_wave, rowc,
+                                                               p);
+            wmax = fmax32(wmax, fmax32(wx, wy));
+        }
+        if (want_wave) {
+            const float bm = block_max(wmax, red);
+            if (tid == 0) {
+                atomicMax(reinterpret_cast<unsigned int*>(A.wave) + t, __float_as_uint(bm));
+                atomicMax(A.R.wave_bits + run, __float_as_uint(bm));
+            }
+        } else {
+            __syncthreads();
+        }
+    }
 }
 
 cudaError_t faces_setup() {
@@ -472,7 +605,27 @@ cudaError_t faces_setup() {
                                                     FACES_SMEM);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(faces_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                     FACES_SMEM);
+    for (auto k : {strips_kernel<true>, strips_kernel<false>}) {
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, STRIP_SMEM);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    }
     return e;
+}
+
+// The resident CTAs a SM of the strip form.
+int strips_occupancy() {
+    int on = 0, off = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&on, strips_kernel<true>, STRIP_THREADS, STRIP_SMEM);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&off, strips_kernel<false>, STRIP_THREADS, STRIP_SMEM);
+    return on < off ? on : off;
+}
+
+// The face pass in its strip form (grid: CTAs; the units are the work list's tiles, two halves each).
+void launch_strips(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s) {
+    if (A.P.second && A.P.sheet && A.P.mirror && A.P.carry)
+        strips_kernel<true><<<grid, STRIP_THREADS, STRIP_SMEM, s>>>(M, A);
+    else
+        strips_kernel<false><<<grid, STRIP_THREADS, STRIP_SMEM, s>>>(M, A);
 }
 
 // The resident CTAs a SM of the face pass (the smaller of its two forms').
@@ -902,6 +1055,10 @@ __device__ void step_settings(const StepArgs& A) {
     if (mine) atomicOr(&any, mine);
     __syncthreads();
     if (threadIdx.x == 0) ctl->any = any;
+    // the wave of each tile of a run that refreshes: the face pass's strip form takes each half's maximum into it
+    if (any & ANY_WAVE)
+        for (int t = threadIdx.x; t < A.ntiles; t += blockDim.x)
+            if (R.flags[A.tile_run[t]] & F_WAVE) A.wave[t] = 0.0f;
 }
 
 __global__ void prestep_kernel(StepArgs A) { step_settings(A); }

@@ -357,18 +357,19 @@ int32_t w2b_build_tables_noalloc(const W2BTableIn* in, const W2BTableOut* out, v
  * with one fixed grid; the tile shape stays the reference's 32 x 32 (its table layout), so what is tuned is the
  * schedule: the face pass's form, CTAs a SM of the face pass and of the update pass, and loop steps a captured graph.
  * Every configuration gives the same results bit for bit. By default the handle tunes online during its first
- * w2b_advance / w2b_advance_runs calls: successive graph launches rotate through six candidates (the default,
- * one face-pass CTA a SM fewer, half the update pass's CTAs a SM, 8 and 32 steps a graph, the strip form), each timed
- * with CUDA events from the end of the launch before it (the host's clock read between graphs included) per loop step
- * that ran; after three launches each the fastest is kept for the handle's life, the default unless another is more
- * than 2 % faster.
- * The strip form of the face pass takes half tiles (16 rows) in CTAs of 256 threads and 54 KB, four a SM: the same
- * faces bit for bit. w2b_loop_tuning(h, 1, ...) starts tuning again; w2b_loop_tuning(h, 0, f, u, s) fixes a
- * configuration with the tile form, w2b_loop_tuning(h, 2, f, u, s) one with the strip form (1 <= f <= the form's
- * resident CTAs a SM, 1 <= u <= the update pass's, 1 <= s <= 64), W2B_EINVAL outside that. w2b_loop_config(h, out)
- * fills out[8]: faces CTAs a SM, update CTAs a SM, steps a graph (while tuning: the next launch's), tuning (1/0), the
- * tile form's and the update pass's resident CTAs a SM, the strip form (1/0), and its resident CTAs a SM. Host-driven
- * steps (w2b_step) take the form and face-pass CTAs the tuner settled on, the tile form while it tunes. */
+ * w2b_advance / w2b_advance_runs calls: successive graph launches rotate through seven candidates (the default,
+ * one face-pass CTA a SM fewer, half the update pass's CTAs a SM, 8 and 32 steps a graph, and the face pass's two
+ * strip forms), each timed with CUDA events from the end of the launch before it (the host's clock read between graphs
+ * included) per loop step that ran; after three launches each the fastest is kept for the handle's life, the default
+ * unless another is more than 2 % faster. The strip forms of the face pass take strips of 16 rows of a tile (CTAs of
+ * 256 threads and 54 KB, four a SM) or of 8 rows (128 threads and 30 KB, seven a SM): the same faces bit for bit.
+ * w2b_loop_tuning(h, 1, ...) starts tuning again; w2b_loop_tuning(h, tune, f, u, s) with tune 0, 2 or 3 fixes a
+ * configuration with the tile form, the 16-row or the 8-row strips (1 <= f <= the form's resident CTAs a SM, 1 <= u <=
+ * the update pass's, 1 <= s <= 64), W2B_EINVAL outside that. w2b_loop_config(h, out) fills out[9]: faces CTAs a SM,
+ * update CTAs a SM, steps a graph (while tuning: the next launch's), tuning (1/0), the tile form's and the update
+ * pass's resident CTAs a SM, the form (0 tiles, else the strip rows), and the 16-row and 8-row strip forms' resident
+ * CTAs a SM. Host-driven steps (w2b_step) take the form and face-pass CTAs the tuner settled on, the tile form while
+ * it tunes. */
 int32_t w2b_loop_tuning(void* handle, int32_t tune, int32_t faces_per_sm, int32_t update_per_sm, int32_t steps);
 int32_t w2b_loop_config(void* handle, int32_t* out);
 

@@ -365,17 +365,20 @@ class B200Backend:
         """The device loop's launch schedule (w2b_loop_config): the face and update passes' CTAs a SM and the loop
         steps a captured graph (while the tuner runs: the next graph launch's), whether it is still tuning, and each
         pass's resident CTAs a SM."""
-        out = np.zeros(8, np.int32)
+        out = np.zeros(9, np.int32)
         _lib.call("w2b_loop_config", self.handle, out.ctypes.data)
         keys = ("faces_per_sm", "update_per_sm", "steps_per_graph", "tuning", "faces_occupancy", "update_occupancy",
-                "strips", "strips_occupancy")  # fmt: skip
+                "strips", "strips16_occupancy", "strips8_occupancy")  # fmt: skip
         return {k: int(v) for k, v in zip(keys, out, strict=True)}
 
     def set_loop(self, tune: bool = True, faces_per_sm: int = 0, update_per_sm: int = 0, steps: int = 0,
-                 strips: bool = False) -> None:  # fmt: skip
+                 strips: int = 0) -> None:  # fmt: skip
         """Start the launch tuner again (``tune``), or fix the device loop's launch schedule (w2b_loop_tuning): the face
-        pass's CTAs a SM in its tile form, or with ``strips`` in its strip form, the update pass's, steps a graph."""
-        code = 1 if tune else (2 if strips else 0)
+        pass's CTAs a SM in its tile form, or with ``strips`` (16 or 8) in its strip form of that many rows, the
+        update pass's CTAs a SM, steps a graph."""
+        if strips not in (0, 8, 16):
+            raise ValueError("strips: 0 (the tile form), 16 or 8")
+        code = 1 if tune else {0: 0, 16: 2, 8: 3}[strips]
         _lib.call("w2b_loop_tuning", self.handle, code, int(faces_per_sm), int(update_per_sm), int(steps))
 
     def max_wave(self) -> float:

@@ -23,8 +23,8 @@ namespace w2b {
     cudaError_t update_setup();                                                     \
     int update_occupancy();                                                         \
     void launch_update(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s); \
-    int strips_occupancy();                                                         \
-    void launch_strips(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s);
+    int strips_occupancy(int rows);                                                 \
+    void launch_strips(int rows, const TMaps& M, const StepArgs& A, int grid, cudaStream_t s);
 namespace exact {
 W2B_PASSES_DECL
 }
@@ -41,8 +41,8 @@ struct Passes {
     cudaError_t (*update_setup)();
     int (*update_occupancy)();
     void (*launch_update)(const TMaps&, const StepArgs&, int, cudaStream_t);
-    int (*strips_occupancy)();
-    void (*launch_strips)(const TMaps&, const StepArgs&, int, cudaStream_t);
+    int (*strips_occupancy)(int);
+    void (*launch_strips)(int, const TMaps&, const StepArgs&, int, cudaStream_t);
 };
 static const Passes EXACT_PASSES = {exact::faces_setup,  exact::launch_probe,     exact::faces_occupancy,
                                     exact::launch_faces, exact::update_setup,     exact::update_occupancy,
@@ -77,9 +77,9 @@ __global__ void bmark_kernel(StepArgs A, int clear_words);
 // order-free integer max); they differ only in time.
 struct LoopConfig {
     int faces_per_sm, update_per_sm, steps;
-    int strips;
+    int strips;  // the face pass's form: 0 whole tiles, else strips of this many rows (16 or 8)
 };
-constexpr int TUNE_CANDIDATES = 6;               // the default, one change of each knob either way, the strip form
+constexpr int TUNE_CANDIDATES = 7;               // the default, one change of each knob either way, two strip forms
 constexpr int FORCED = TUNE_CANDIDATES;          // the slot of a configuration the caller fixes
 constexpr int TUNE_SAMPLES = 3;                  // timed graph launches a candidate before the tuner settles
 constexpr int MAX_GRAPH_STEPS = 64;
@@ -131,7 +131,7 @@ struct Handle {
     int step_blocks = 148;   // resident CTAs of the update pass
     int faces_blocks = 296;  // resident CTAs of the face pass
     int faces_occ = 2, update_occ = 1;  // resident CTAs a SM of the two passes
-    int strips_occ = 4;                 // resident CTAs a SM of the face pass's strip form
+    int strips16_occ = 4, strips8_occ = 7;  // resident CTAs a SM of the face pass's strip forms
     TMaps tmaps;
     unsigned version = 0;   // bumped whenever a graph would capture stale arguments
     Loop loop;
@@ -294,24 +294,27 @@ static int build_tmaps(Handle& H) {
         own(&H.tmaps.mx[p], B.mx[p]);
         own(&H.tmaps.my[p], B.my[p]);
     }
-    // the strip form's boxes: 40 x 20 (half a tile and its halo), 32 x 16 for the momenta
-    auto strip = [&](CUtensorMap* m, const float* q) {
-        if (st == W2B_OK) st = encode_2d(enc, m, q, H.g, H.L, 40, 20);
-    };
-    auto strip_own = [&](CUtensorMap* m, const float* q) {
-        if (st == W2B_OK) st = encode_2d(enc, m, q, H.g, H.L, 32, 16);
-    };
-    strip(&H.tmaps.sd, B.d);
-    strip(&H.tmaps.sqx, B.qx);
-    strip(&H.tmaps.sqy, B.qy);
-    strip(&H.tmaps.szcx, B.zcx);
-    strip(&H.tmaps.szcy, B.zcy);
-    for (int p = 0; p < 2; ++p) {
-        strip(&H.tmaps.sh[p], B.h[p]);
-        strip(&H.tmaps.su[p], B.u[p]);
-        strip(&H.tmaps.sv[p], B.v[p]);
-        strip_own(&H.tmaps.smx[p], B.mx[p]);
-        strip_own(&H.tmaps.smy[p], B.my[p]);
+    // the strip forms' boxes: 40 x (rows + 4) (the strip and its halo), 32 x rows for the momenta
+    for (const int rows : {16, 8}) {
+        StripMaps& S = rows == 16 ? H.tmaps.s16 : H.tmaps.s8;
+        auto strip = [&](CUtensorMap* m, const float* q) {
+            if (st == W2B_OK) st = encode_2d(enc, m, q, H.g, H.L, 40, (uint32_t)rows + 4);
+        };
+        auto strip_own = [&](CUtensorMap* m, const float* q) {
+            if (st == W2B_OK) st = encode_2d(enc, m, q, H.g, H.L, 32, (uint32_t)rows);
+        };
+        strip(&S.d, B.d);
+        strip(&S.qx, B.qx);
+        strip(&S.qy, B.qy);
+        strip(&S.zcx, B.zcx);
+        strip(&S.zcy, B.zcy);
+        for (int p = 0; p < 2; ++p) {
+            strip(&S.h[p], B.h[p]);
+            strip(&S.u[p], B.u[p]);
+            strip(&S.v[p], B.v[p]);
+            strip_own(&S.mx[p], B.mx[p]);
+            strip_own(&S.my[p], B.my[p]);
+        }
     }
     return st;
 }
@@ -340,7 +343,8 @@ static void init_loop(Handle& H) {
     if (U > 1) L.cand[L.ncand++] = {F, (U + 1) / 2, 16, 0};
     L.cand[L.ncand++] = {F, U, 8, 0};
     L.cand[L.ncand++] = {F, U, 32, 0};
-    L.cand[L.ncand++] = {H.strips_occ, U, 16, 1};
+    L.cand[L.ncand++] = {H.strips16_occ, U, 16, 16};
+    L.cand[L.ncand++] = {H.strips8_occ, U, 16, 8};
     L.cand[FORCED] = L.cand[0];
     for (int c = 0; c < TUNE_CANDIDATES; ++c) {
         L.sec[c] = 0.0;
@@ -372,10 +376,12 @@ static int set_passes(Handle& H) {
             return cuda_status(cudaGetLastError(), "pass setup");
     }
     const Passes& X = passes(H.P);
-    const int occ = X.update_occupancy(), focc = X.faces_occupancy(), socc = X.strips_occupancy();
+    const int occ = X.update_occupancy(), focc = X.faces_occupancy();
+    const int s16 = X.strips_occupancy(16), s8 = X.strips_occupancy(8);
     H.update_occ = occ > 0 ? occ : 1;
     H.faces_occ = focc > 0 ? focc : 1;
-    H.strips_occ = socc > 0 ? socc : 1;
+    H.strips16_occ = s16 > 0 ? s16 : 1;
+    H.strips8_occ = s8 > 0 ? s8 : 1;
     H.step_blocks = H.sms * H.update_occ;
     H.faces_blocks = H.sms * H.faces_occ;
     init_loop(H);
@@ -387,8 +393,8 @@ static int set_passes(Handle& H) {
 static void launch_faces_host(Handle& H, const StepArgs& A, int n, cudaStream_t s) {
     const LoopConfig& C = H.loop.cand[H.loop.chosen];
     if (!H.loop.tuning && C.strips) {
-        const int g = H.sms * C.faces_per_sm;
-        passes(H.P).launch_strips(H.tmaps, A, 2 * n < g ? 2 * n : g, s);
+        const int g = H.sms * C.faces_per_sm, units = (TILE / C.strips) * n;
+        passes(H.P).launch_strips(C.strips, H.tmaps, A, units < g ? units : g, s);
     } else {
         passes(H.P).launch_faces(H.tmaps, A, faces_grid(H, n), s);
     }
@@ -404,7 +410,7 @@ static int launch_loop_step(Handle& H, const LoopConfig& C, cudaStream_t s) {
     const int fgrid = H.sms * C.faces_per_sm, ugrid = H.sms * C.update_per_sm;
     const Passes& X = passes(H.P);
     if (C.strips)
-        X.launch_strips(H.tmaps, A, 2 * tiles < fgrid ? 2 * tiles : fgrid, s);
+        X.launch_strips(C.strips, H.tmaps, A, (TILE / C.strips) * tiles < fgrid ? (TILE / C.strips) * tiles : fgrid, s);
     else
         X.launch_faces(H.tmaps, A, tiles < fgrid ? tiles : fgrid, s);
     X.launch_update(H.tmaps, A, tiles < ugrid ? tiles : ugrid, s);
@@ -995,9 +1001,10 @@ int32_t w2b_loop_tuning(void* handle, int32_t tune, int32_t faces_per_sm, int32_
         init_loop(*H);
         return W2B_OK;
     }
-    const int strips = tune == 2;
-    if (tune != 0 && tune != 2) return W2B_EINVAL;
-    if (faces_per_sm < 1 || faces_per_sm > (strips ? H->strips_occ : H->faces_occ) || update_per_sm < 1 ||
+    if (tune < 0 || tune > 3) return W2B_EINVAL;
+    const int strips = tune == 2 ? 16 : (tune == 3 ? 8 : 0);
+    const int occ = strips == 16 ? H->strips16_occ : (strips == 8 ? H->strips8_occ : H->faces_occ);
+    if (faces_per_sm < 1 || faces_per_sm > occ || update_per_sm < 1 ||
         update_per_sm > H->update_occ || steps < 1 || steps > MAX_GRAPH_STEPS)
         return W2B_EINVAL;
     L.cand[FORCED] = {faces_per_sm, update_per_sm, steps, strips};
@@ -1019,7 +1026,8 @@ int32_t w2b_loop_config(void* handle, int32_t* out) {
     out[4] = H->faces_occ;
     out[5] = H->update_occ;
     out[6] = C.strips;
-    out[7] = H->strips_occ;
+    out[7] = H->strips16_occ;
+    out[8] = H->strips8_occ;
     return W2B_OK;
 }
 

@@ -157,12 +157,15 @@ struct StepArgs {
 // Tensor maps of the NATIVE state arrays for the face pass's TMA boxes: 40 x 36 floats (the tile, two cells of halo
 // north and south, four west and east so that the box's first column stays 16-byte aligned), and 32 x 32 for the
 // momenta, which the face pass reads at own faces only. Ping-pong pairs have one map a half.
+// The strip forms of the face pass (strips of H rows of a tile): 40 x (H + 4) boxes, and 32 x H for the momenta.
+struct StripMaps {
+    CUtensorMap d, h[2], u[2], v[2], qx, qy, zcx, zcy, mx[2], my[2];
+};
 struct TMaps {
     CUtensorMap d, h[2], u[2], v[2], qx, qy, om, zcx, zcy, mx[2], my[2];
     CUtensorMap qx1, qy1;  // 40 x 36 boxes for the update pass
     CUtensorMap res, src;  // 32 x 32 boxes
-    // the strip form of the face pass (half a tile, 16 rows): 40 x 20 boxes, and 32 x 16 for the momenta
-    CUtensorMap sd, sh[2], su[2], sv[2], sqx, sqy, szcx, szcy, smx[2], smy[2];
+    StripMaps s16, s8;     // strips of 16 and of 8 rows
 };
 
 // ------------------------------------------------------------------ float32 helpers

@@ -48,14 +48,15 @@ struct TileImage {
     static constexpr int BOX = w2b::W2B_ARITH::BOX, ZCX = F_ZCX, ZCY = F_ZCY, M = SM_M, ST = SM_ST, S = TILE2;
     static constexpr bool OM = true;
 };
-constexpr int SROWS = 16, SBOXH = SROWS + 4, SBOX = BOXW * SBOXH, SNBOX = 8, STILE = TILE * SROWS;
+template <int H>
 struct StripImage {
-    static constexpr int BOX = SBOX, ZCX = 6, ZCY = 7, M = SNBOX * SBOX, ST = SNBOX * SBOX + 2 * STILE, S = STILE;
+    static constexpr int BOX = BOXW * (H + 4), ZCX = 6, ZCY = 7, M = 8 * BOX, ST = 8 * BOX + 2 * TILE * H, S = TILE * H;
     static constexpr bool OM = false;
+    static constexpr int FLOATS = ST + 12 * S;
+    static constexpr int SMEM = FLOATS * 4;        // 54,272 bytes for 16 rows (four CTAs a SM), 29,696 for 8 (seven)
+    static constexpr int THREADS = 16 * H;         // a warp two rows
+    static constexpr int CTAS = H == 16 ? 4 : 7;   // resident CTAs a SM the launch bound plans for
 };
-constexpr int STRIP_FLOATS = StripImage::ST + 12 * STILE;
-constexpr int STRIP_SMEM = STRIP_FLOATS * 4;  // 54,272 bytes: four CTAs a SM
-constexpr int STRIP_THREADS = 256;
 
 // What the first part of a face hands to the rest: the row's quad (its load is issued in part A and consumed after
 // the table-free momentum terms), the face depth, and the table row with the upwind choice, the live flag and the
@@ -494,22 +495,27 @@ void launch_probe(const StepArgs& A, int t, float dt, float* out, cudaStream_t s
     probe_kernel<<<1, 1024, SM_FLOATS * 4, s>>>(A, t, dt, out);
 }
 
-// The strip form of the face pass: the same faces, half a tile at a time. A unit of work is one 16-row half of a tile of
-// the work list (2 nwork units); a CTA of 256 threads (8 warps, a warp a strip row, two rows a warp) stages the strip
-// with TMA as eight 40 x 20 boxes, its momenta as 32 x 16 boxes and its twelve static face scalars as 2 KB bulk copies,
-// 54 KB in all, so that four CTAs share a SM and one waits for its copies while three compute (the tile form's two
-// CTAs of 109 KB leave a SM idle whenever both wait). The plan shares, wanted on refresh steps only, are read from
+// The strip forms of the face pass: the same faces, a strip of H rows of a tile at a time (H = 16: halves, H = 8:
+// quarters). A unit of work is one strip of a tile of the work list (32 / H units a tile); a CTA of 16 H threads (H / 2
+// warps, two rows a warp) stages the strip with TMA as eight 40 x (H + 4) boxes, its momenta as 32 x H boxes and its
+// twelve static face scalars as bulk copies: 54 KB for 16 rows, so that four CTAs share a SM, 30 KB for 8 rows, seven.
+// While one CTA waits for its copies the others compute (the tile form's two CTAs of 109 KB leave a SM idle whenever
+// both wait). The plan shares, wanted on refresh steps only, are read from
 // global memory. A face's arithmetic is the tile form's, bit for bit. On refresh steps each strip's wave maximum goes
 // to its tile's entry and its run's maximum by integer atomic maxima on the float bits.
-template <bool ON>
-__global__ void __launch_bounds__(STRIP_THREADS, 4) strips_kernel(const __grid_constant__ TMaps M, StepArgs A) {
+template <int H, bool ON>
+__global__ void __launch_bounds__(StripImage<H>::THREADS, StripImage<H>::CTAS)
+    strips_kernel(const __grid_constant__ TMaps M, StepArgs A) {
+    using L = StripImage<H>;
+    constexpr int PER = TILE / H;  // strips a tile
+    const StripMaps& SM_ = H == 16 ? M.s16 : M.s8;
     extern __shared__ __align__(128) float sm[];
     __shared__ __align__(8) uint64_t bar;
     __shared__ float red[32];
     __shared__ float rowc[2 * 64 + 1];
     Ctl* ctl = A.ctl;
     if (!(ctl->any & ANY_RUN)) return;
-    const int nunits = 2 * ctl->nwork;
+    const int nunits = PER * ctl->nwork;
     const int tid = threadIdx.x;
     if (tid == 0) {
         mbar_init(&bar, 1);
@@ -532,8 +538,8 @@ __global__ void __launch_bounds__(STRIP_THREADS, 4) strips_kernel(const __grid_c
     uint32_t phase = 0;
     const int lane = tid & 31, warp = tid >> 5;
     for (int u = blockIdx.x; u < nunits; u += gridDim.x) {
-        const int t = A.list[u >> 1];
-        const int row0 = (u & 1) * SROWS;
+        const int t = A.list[u / PER];
+        const int row0 = (u % PER) * H;
         const int run = A.tile_run[t];
         const int flags = A.R.flags[run];
         if (!(flags & F_RUN)) continue;  // the tile's run has finished: uniform over the CTA
@@ -545,21 +551,20 @@ __global__ void __launch_bounds__(STRIP_THREADS, 4) strips_kernel(const __grid_c
         const int ts = table_of(A, t);
         if (tid == 0) {
             fence_proxy_async();
-            mbar_expect_tx(&bar, (uint32_t)STRIP_SMEM);
+            mbar_expect_tx(&bar, (uint32_t)L::SMEM);
             const int x0 = ti * TILE + GX - 4, y0 = tj * TILE + GY + row0 - 2;
-            tma_load_2d(sm + F_D * SBOX, &M.sd, x0, y0, &bar);
-            tma_load_2d(sm + F_H * SBOX, &M.sh[p], x0, y0, &bar);
-            tma_load_2d(sm + F_U * SBOX, &M.su[p], x0, y0, &bar);
-            tma_load_2d(sm + F_V * SBOX, &M.sv[p], x0, y0, &bar);
-            tma_load_2d(sm + F_QX * SBOX, &M.sqx, x0, y0, &bar);
-            tma_load_2d(sm + F_QY * SBOX, &M.sqy, x0, y0, &bar);
-            tma_load_2d(sm + StripImage::ZCX * SBOX, &M.szcx, x0, y0, &bar);
-            tma_load_2d(sm + StripImage::ZCY * SBOX, &M.szcy, x0, y0, &bar);
-            tma_load_2d(sm + StripImage::M, &M.smx[p], x0 + 4, y0 + 2, &bar);
-            tma_load_2d(sm + StripImage::M + STILE, &M.smy[p], x0 + 4, y0 + 2, &bar);
+            tma_load_2d(sm + F_D * L::BOX, &SM_.d, x0, y0, &bar);
+            tma_load_2d(sm + F_H * L::BOX, &SM_.h[p], x0, y0, &bar);
+            tma_load_2d(sm + F_U * L::BOX, &SM_.u[p], x0, y0, &bar);
+            tma_load_2d(sm + F_V * L::BOX, &SM_.v[p], x0, y0, &bar);
+            tma_load_2d(sm + F_QX * L::BOX, &SM_.qx, x0, y0, &bar);
+            tma_load_2d(sm + F_QY * L::BOX, &SM_.qy, x0, y0, &bar);
+            tma_load_2d(sm + L::ZCX * L::BOX, &SM_.zcx, x0, y0, &bar);
+            tma_load_2d(sm + L::ZCY * L::BOX, &SM_.zcy, x0, y0, &bar);
+            tma_load_2d(sm + L::M, &SM_.mx[p], x0 + 4, y0 + 2, &bar);
+            tma_load_2d(sm + L::M + L::S, &SM_.my[p], x0 + 4, y0 + 2, &bar);
             for (int f = 0; f < 12; ++f)
-                bulk_load(sm + StripImage::ST + f * STILE, statics[f] + (size_t)ts * TILE2 + row0 * TILE, STILE * 4,
-                          &bar);
+                bulk_load(sm + L::ST + f * L::S, statics[f] + (size_t)ts * TILE2 + row0 * TILE, L::S * 4, &bar);
         }
         const bool ok = mbar_wait(&bar, phase);
         phase ^= 1u;
@@ -573,17 +578,17 @@ __global__ void __launch_bounds__(STRIP_THREADS, 4) strips_kernel(const __grid_c
         float wmax = 0.0f;
 #pragma unroll 1
         for (int c = 0; c < 2; ++c) {
-            const int js = warp + 8 * c, ii = lane;  // the row in the strip, and in the tile
+            const int js = warp + (H / 2) * c, ii = lane;  // the row in the strip, and in the tile
             const int jj = row0 + js;
             const int sl = js * TILE + ii, local = jj * TILE + ii;
             const int b = (js + 2) * BOXW + ii + 4;
             const int k = base + jj * A.px + ii;
             FaceA fx, fy;
-            face_a<0, ON, StripImage>(sm, b, sl, local, A, ts, fx);
-            face_a<1, ON, StripImage>(sm, b, sl, local, A, ts, fy);
-            const float wx = face_bc<0, false, ON, StripImage>(sm, b, sl, local, k, A, ts, fx, dt, dx, want_wave, rowc,
+            face_a<0, ON, L>(sm, b, sl, local, A, ts, fx);
+            face_a<1, ON, L>(sm, b, sl, local, A, ts, fy);
+            const float wx = face_bc<0, false, ON, L>(sm, b, sl, local, k, A, ts, fx, dt, dx, want_wave, rowc,
                                                                p);
-            const float wy = face_bc<1, false, ON, StripImage>(sm, b, sl, local, k, A, ts, fy, dt, dx, want_wave, rowc,
+            const float wy = face_bc<1, false, ON, L>(sm, b, sl, local, k, A, ts, fy, dt, dx, want_wave, rowc,
                                                                p);
             wmax = fmax32(wmax, fmax32(wx, wy));
         }
@@ -605,27 +610,51 @@ cudaError_t faces_setup() {
                                                     FACES_SMEM);
     if (e == cudaSuccess) e = cudaFuncSetAttribute(faces_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                     FACES_SMEM);
-    for (auto k : {strips_kernel<true>, strips_kernel<false>}) {
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, STRIP_SMEM);
+    for (auto k : {strips_kernel<16, true>, strips_kernel<16, false>}) {
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, StripImage<16>::SMEM);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
+    }
+    for (auto k : {strips_kernel<8, true>, strips_kernel<8, false>}) {
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, StripImage<8>::SMEM);
         if (e == cudaSuccess) e = cudaFuncSetAttribute(k, cudaFuncAttributePreferredSharedMemoryCarveout, 100);
     }
     return e;
 }
 
-// The resident CTAs a SM of the strip form.
-int strips_occupancy() {
+// The resident CTAs a SM of the strip form of `rows` rows (16 or 8).
+int strips_occupancy(int rows) {
     int on = 0, off = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&on, strips_kernel<true>, STRIP_THREADS, STRIP_SMEM);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&off, strips_kernel<false>, STRIP_THREADS, STRIP_SMEM);
+    if (rows == 16) {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&on, strips_kernel<16, true>, StripImage<16>::THREADS,
+                                                      StripImage<16>::SMEM);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&off, strips_kernel<16, false>, StripImage<16>::THREADS,
+                                                      StripImage<16>::SMEM);
+    } else {
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&on, strips_kernel<8, true>, StripImage<8>::THREADS,
+                                                      StripImage<8>::SMEM);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&off, strips_kernel<8, false>, StripImage<8>::THREADS,
+                                                      StripImage<8>::SMEM);
+    }
     return on < off ? on : off;
 }
 
-// The face pass in its strip form (grid: CTAs; the units are the work list's tiles, two halves each).
-void launch_strips(const TMaps& M, const StepArgs& A, int grid, cudaStream_t s) {
-    if (A.P.second && A.P.sheet && A.P.mirror && A.P.carry)
-        strips_kernel<true><<<grid, STRIP_THREADS, STRIP_SMEM, s>>>(M, A);
-    else
-        strips_kernel<false><<<grid, STRIP_THREADS, STRIP_SMEM, s>>>(M, A);
+// The face pass in its strip form of `rows` rows (16 or 8); grid: CTAs (the units are the work list's tiles, 32 /
+// rows strips each).
+void launch_strips(int rows, const TMaps& M, const StepArgs& A, int grid, cudaStream_t s) {
+    const bool on = A.P.second && A.P.sheet && A.P.mirror && A.P.carry;
+    if (rows == 16) {
+        if (on)
+            strips_kernel<16, true><<<grid, StripImage<16>::THREADS, StripImage<16>::SMEM, s>>>(M, A);
+        else
+            strips_kernel<16, false><<<grid, StripImage<16>::THREADS, StripImage<16>::SMEM, s>>>(M, A);
+    } else {
+        if (on)
+            strips_kernel<8, true><<<grid, StripImage<8>::THREADS, StripImage<8>::SMEM, s>>>(M, A);
+        else
+            strips_kernel<8, false><<<grid, StripImage<8>::THREADS, StripImage<8>::SMEM, s>>>(M, A);
+    }
 }
 
 // The resident CTAs a SM of the face pass (the smaller of its two forms').

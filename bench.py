@@ -914,7 +914,9 @@ def main() -> None:
     hbm, peak_kind = peaks()
     achieved = ALG_FACES * tile_cells / (faces / 1e3) / 1e9
     traffic = FACES_DRAM_BYTES_PER_CELL * tile_cells
-    roofline = {"kernel": f"{args.arith}::faces_kernel", "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
+    form = b.loop_config()["strips"]
+    kernel = f"{args.arith}::strips_kernel<{form}>" if form else f"{args.arith}::faces_kernel"
+    roofline = {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": traffic,
                 "alg_bytes_per_cell": ALG_FACES, "launch_ms": faces,
                 "update_kernel_ms": statistics.mean(update_ms),

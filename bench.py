@@ -8,11 +8,14 @@ reference's "adaptive_active off" headline mode); the envelope every 4 steps and
 as the reference's monitor takes them. A step is one time step of the whole grid (the device-resident loop,
 graph-captured). Inputs stay resident in HBM (about 15 GB, far beyond the 126 MB L2).
 
-JSON line (rank 0): value = domain cell-steps per second over all ranks (ranks run independent replicas: weak
-scaling, no collective in the data path); roofline of the dominant kernel (the face pass) from CUDA events;
-cpu_baseline = the oracle (a C restatement of the reference's CPU step) on a bounded block of the same workload;
-e2e = the same metric through the C-ABI with host buffers (a source window's rain uploaded from pinned memory, the
-loop run, the clock read back, per 30 s window as the reference's run driver does).
+The step is the fast build by default (``--arith``), the launch schedule and the face pass's form (tiles or strips)
+chosen by the library's tuner before the timed steps. JSON line (rank 0): value = domain cell-steps per second over
+all ranks (ranks run independent replicas: weak scaling, no collective in the data path); roofline of the dominant
+kernel (the face pass) from CUDA events; parity = the timed build against the oracle on a block of the workload;
+cpu_baseline = the oracle (a C restatement of the reference's CPU step) on that block; e2e = the same metric through
+the C-ABI with host buffers (per 30 s window, as the reference's run driver and monitor take a run: the window's rain
+uploaded from pinned memory, the window stepped, the clock, active list, design-line discharge, outfall volume and
+storage read back; the envelope maps at the end); sweep = the critical-duration search at a reduced size.
 
 ``--impl reference`` times the reference's CPU step (its restatement, the oracle, with every host thread) on the
 same bounded block and prints the same line with "impl": "reference".
@@ -364,7 +367,7 @@ def full_run(args) -> None:
     grid = TileGrid.from_mask(np.ones((args.n, args.n), bool), 0.0, 0.0, c.dx)
     tables = build_tables(grid, ArrayBed(c.z, c.dx / c.k), Tables(), c.manning, device=dev)
     del c.z
-    m = Model(tables, Numerics())
+    m = Model(tables, Numerics(arithmetic=args.arith))
     rows, cols = c.boundary_cells()
     cells = state_index(grid, rows, cols).astype(np.int32)
     nb = cells.size
@@ -480,7 +483,7 @@ def ensemble_run(args) -> None:
     inputs = [ensemble_inputs(specs[r], dev) for r in mine]
     torch.cuda.synchronize(dev)
     setup = time.perf_counter() - t0
-    num = Numerics()
+    num = Numerics(arithmetic=args.arith)
     t_end = t_all[mine]
     storms = [specs[r].storm() for r in mine]
     cells = np.array([int(i[0].mask.sum()) for i in inputs], np.float64)
@@ -687,7 +690,7 @@ def config2_run(args) -> None:
     tables = build_tables(grid, ArrayBed(torch.as_tensor(c.z, device=dev), c.dx / c.k), Tables(), c.manning,
                           crest=c.crest, device=dev)  # fmt: skip
     del c.z
-    m = Model(tables, Numerics())
+    m = Model(tables, Numerics(arithmetic=args.arith))
     rows, cols = c.outfall
     cells = state_index(grid, rows, cols).astype(np.int32)
     nb = cells.size

@@ -63,6 +63,9 @@ def parse():
                    help="the step's build: fast (the default: FMA contraction, approximate division, square root and "
                         "powers in the face pass, held to the step's accuracy bounds against the oracle and the FP64 "
                         "run) or exact (the reference's float32 bits)")
+    p.add_argument("--form", default="tuned", choices=("tuned", "tiles", "strips16", "strips8"),
+                   help="the face pass's form: the one the launch tuner keeps (the default), or fixed (the tile form, or "
+                        "strips of 16 or 8 rows, each at its resident CTAs a SM)")
     p.add_argument("--parity-steps", type=int, default=200,
                    help="steps of the CUDA path against the oracle on the CPU sample block (0: none)")
     p.add_argument("--n", type=int, default=4096, help="domain side in cells (configuration 3: 4096)")
@@ -877,6 +880,11 @@ def main() -> None:
 
     # warm-up: the graph capture and the first steps; then the launch tuner settles (its candidate schedules give the
     # same bits and differ only in time), so the timed steps run the schedule it kept
+    if args.form != "tuned":
+        lc = b.loop_config()
+        strips = {"tiles": 0, "strips16": 16, "strips8": 8}[args.form]
+        occ = {0: lc["faces_occupancy"], 16: lc["strips16_occupancy"], 8: lc["strips8_occupancy"]}[strips]
+        b.set_loop(False, occ, lc["update_occupancy"], 16, strips)
     m.run(1e12, maxima=maxima, tally=tally, max_steps=max(args.warmup, 3))
     tune_steps = 0
     while b.loop_config()["tuning"] and tune_steps < 4096:

@@ -131,7 +131,7 @@ struct Handle {
     int step_blocks = 148;   // resident CTAs of the update pass
     int faces_blocks = 296;  // resident CTAs of the face pass
     int faces_occ = 2, update_occ = 1;  // resident CTAs a SM of the two passes
-    int strips16_occ = 4, strips8_occ = 7;  // resident CTAs a SM of the face pass's strip forms
+    int strips16_occ = 4, strips8_occ = 8;  // resident CTAs a SM of the face pass's strip forms
     TMaps tmaps;
     unsigned version = 0;   // bumped whenever a graph would capture stale arguments
     Loop loop;
@@ -294,24 +294,26 @@ static int build_tmaps(Handle& H) {
         own(&H.tmaps.mx[p], B.mx[p]);
         own(&H.tmaps.my[p], B.my[p]);
     }
-    // the strip forms' boxes: 40 x (rows + 4) (the strip and its halo), 32 x rows for the momenta
+    // the strip forms' boxes, 40 columns of the rows the face arithmetic reads around a strip of `rows` rows: the
+    // velocities rows + 4 (two above, two below), the y discharge rows + 2, the x lip rows, depth, mean depth, x
+    // discharge and y lip rows + 1 (one above); 32 x rows for the momenta
     for (const int rows : {16, 8}) {
         StripMaps& S = rows == 16 ? H.tmaps.s16 : H.tmaps.s8;
-        auto strip = [&](CUtensorMap* m, const float* q) {
-            if (st == W2B_OK) st = encode_2d(enc, m, q, H.g, H.L, 40, (uint32_t)rows + 4);
+        auto strip = [&](CUtensorMap* m, const float* q, int extra) {
+            if (st == W2B_OK) st = encode_2d(enc, m, q, H.g, H.L, 40, (uint32_t)(rows + extra));
         };
         auto strip_own = [&](CUtensorMap* m, const float* q) {
             if (st == W2B_OK) st = encode_2d(enc, m, q, H.g, H.L, 32, (uint32_t)rows);
         };
-        strip(&S.d, B.d);
-        strip(&S.qx, B.qx);
-        strip(&S.qy, B.qy);
-        strip(&S.zcx, B.zcx);
-        strip(&S.zcy, B.zcy);
+        strip(&S.d, B.d, 1);
+        strip(&S.qx, B.qx, 1);
+        strip(&S.qy, B.qy, 2);
+        strip(&S.zcx, B.zcx, 0);
+        strip(&S.zcy, B.zcy, 1);
         for (int p = 0; p < 2; ++p) {
-            strip(&S.h[p], B.h[p]);
-            strip(&S.u[p], B.u[p]);
-            strip(&S.v[p], B.v[p]);
+            strip(&S.h[p], B.h[p], 1);
+            strip(&S.u[p], B.u[p], 4);
+            strip(&S.v[p], B.v[p], 4);
             strip_own(&S.mx[p], B.mx[p]);
             strip_own(&S.my[p], B.my[p]);
         }

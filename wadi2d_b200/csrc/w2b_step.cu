@@ -40,23 +40,51 @@ constexpr int SM_FLOATS = SM_ST + 12 * TILE2;
 constexpr int FACES_SMEM = SM_FLOATS * 4;  // 109,184 bytes: two CTAs a SM
 constexpr int FACES_THREADS = 512;
 
-// The two images the face helpers read. A whole tile (the face pass and the probe): nine 40 x 36 boxes, the plan
-// share among them. A strip (half a tile, 16 rows: the strip form of the face pass): eight 40 x 20 boxes, the plan
-// share read from global memory on the refresh steps that want it. S is the stride of a static face scalar's (and of
-// a momentum's) array in the image: 1,024 floats for a tile, 512 for a strip.
+// The two images the face helpers read. off(f) is the offset of state field f's array as the helpers index it, by
+// box index b (b's row 0 is two rows above the tile's or strip's first row, its column 0 four columns west of the
+// first column; a row is BOXW floats). A whole tile (the face pass and the probe): nine 40 x 36 boxes, the plan share
+// among them. A strip (the strip forms of the face pass): each state field's box holds only the rows the face
+// arithmetic reads, the plan share is read from global memory on the refresh steps that want it. S is the stride of a
+// static face scalar's (and of a momentum's) array in the image: 1,024 floats for a tile, 32 H for a strip.
 struct TileImage {
-    static constexpr int BOX = w2b::W2B_ARITH::BOX, ZCX = F_ZCX, ZCY = F_ZCY, M = SM_M, ST = SM_ST, S = TILE2;
+    static constexpr int M = SM_M, ST = SM_ST, S = TILE2;
     static constexpr bool OM = true;
+    __host__ __device__ static constexpr int off(int f) { return f * BOX; }
 };
+__host__ __device__ constexpr int pad32(int n) { return (n + 31) / 32 * 32; }  // floats, to a 128-byte boundary
 template <int H>
 struct StripImage {
-    static constexpr int BOX = BOXW * (H + 4), ZCX = 6, ZCY = 7, M = 8 * BOX, ST = 8 * BOX + 2 * TILE * H, S = TILE * H;
+    // The rows of each field's box around a strip of H rows, from the face arithmetic's reads (b - S, b, b + S,
+    // b +- 2 S, b +- PP, b +- 2 PP of face_in, face_a, face_bc): the velocities two rows above to two below; depth,
+    // mean depth, x discharge and the y lip one row above to the last row; the y discharge one above to one below;
+    // the x lip the strip's own rows.
+    static constexpr int R_UV = H + 4, R_QY = H + 2, R_ZCX = H, R_1 = H + 1;
+    // each box's region, 128-byte aligned, in the order u v d h qx qy zcx zcy (u first: every offset is >= 0)
+    static constexpr int S_U = 0, S_V = S_U + pad32(BOXW * R_UV), S_D = S_V + pad32(BOXW * R_UV);
+    static constexpr int S_H = S_D + pad32(BOXW * R_1), S_QX = S_H + pad32(BOXW * R_1);
+    static constexpr int S_QY = S_QX + pad32(BOXW * R_1), S_ZCX = S_QY + pad32(BOXW * R_QY);
+    static constexpr int S_ZCY = S_ZCX + pad32(BOXW * R_ZCX), S_END = S_ZCY + pad32(BOXW * R_1);
+    static constexpr int M = S_END, ST = S_END + 2 * TILE * H, S = TILE * H;
     static constexpr bool OM = false;
     static constexpr int FLOATS = ST + 12 * S;
-    static constexpr int SMEM = FLOATS * 4;        // 54,272 bytes for 16 rows (four CTAs a SM), 29,696 for 8 (seven)
+    static constexpr int SMEM = FLOATS * 4;        // 51,840 bytes for 16 rows (four CTAs a SM), 27,264 for 8 (eight)
+    // the bytes the strip's copies bring (the regions without their padding)
+    static constexpr int BYTES = 4 * (BOXW * (2 * R_UV + 4 * R_1 + R_QY + R_ZCX) + 14 * TILE * H);
     static constexpr int THREADS = 16 * H;         // a warp two rows
-    static constexpr int CTAS = H == 16 ? 4 : 7;   // resident CTAs a SM the launch bound plans for
+    static constexpr int CTAS = H == 16 ? 4 : 8;   // resident CTAs a SM the launch bound plans for
+    __host__ __device__ static constexpr int off(int f) {
+        return f == F_U   ? S_U
+             : f == F_V   ? S_V
+             : f == F_D   ? S_D - BOXW
+             : f == F_H   ? S_H - BOXW
+             : f == F_QX  ? S_QX - BOXW
+             : f == F_QY  ? S_QY - BOXW
+             : f == F_ZCX ? S_ZCX - 2 * BOXW
+                          : S_ZCY - BOXW;
+    }
 };
+static_assert(StripImage<8>::SMEM == 27264 && StripImage<16>::SMEM == 51840, "strip image sizes");
+static_assert(StripImage<8>::off(F_D) >= 0 && StripImage<8>::off(F_ZCX) >= 0, "strip offsets");
 
 // What the first part of a face hands to the rest: the row's quad (its load is issued in part A and consumed after
 // the table-free momentum terms), the face depth, and the table row with the upwind choice, the live flag and the
@@ -77,8 +105,8 @@ struct FaceIn {
 template <int AX, class L>
 __device__ __forceinline__ FaceIn face_in(const float* sm, int b, int sl) {
     constexpr int S = AX == 0 ? 1 : BOXW;
-    const float* D = sm + F_D * L::BOX;
-    const float* U = sm + (AX == 0 ? F_U : F_V) * L::BOX;
+    const float* D = sm + L::off(F_D);
+    const float* U = sm + L::off(AX == 0 ? F_U : F_V);
     const float* st = sm + L::ST + AX * 6 * L::S;
     FaceIn I;
     I.e_l = D[b - S] - st[0 * L::S + sl];
@@ -108,7 +136,7 @@ __device__ __forceinline__ void face_a(const float* sm, int b, int sl, int local
     const float top = st[4 * L::S + sl];
     float eface = eup;
     if ((ON || P.carry) && cwf == 0.0f) {
-        const float* ZC = sm + (AX == 0 ? L::ZCX : L::ZCY) * L::BOX;
+        const float* ZC = sm + L::off(AX == 0 ? F_ZCX : F_ZCY);
         const float dz = from_left ? ZC[b - S] - st[0 * L::S + sl] : ZC[b] - st[1 * L::S + sl];
         if (dz > 1e-6f) {
             float phi = qdiv(eup - 2.0f * dz, 2.0f * dz);
@@ -147,11 +175,11 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int sl, int loc
     }
     const float ZERO = 0.0f, HALF = 0.5f, ONE = 1.0f;
     const float span = dx;
-    const float* H = sm + F_H * L::BOX;
-    const float* U = sm + (AX == 0 ? F_U : F_V) * L::BOX;
-    const float* VP = sm + (AX == 0 ? F_V : F_U) * L::BOX;
-    const float* Q = sm + (AX == 0 ? F_QX : F_QY) * L::BOX;
-    const float* QP = sm + (AX == 0 ? F_QY : F_QX) * L::BOX;
+    const float* H = sm + L::off(F_H);
+    const float* U = sm + L::off(AX == 0 ? F_U : F_V);
+    const float* VP = sm + L::off(AX == 0 ? F_V : F_U);
+    const float* Q = sm + L::off(AX == 0 ? F_QX : F_QY);
+    const float* QP = sm + L::off(AX == 0 ? F_QY : F_QX);
     const float* st = sm + L::ST + AX * 6 * L::S;
     const FaceIn I = face_in<AX, L>(sm, b, sl);
     const bool from_left = (F.bits & FA_LEFT) != 0;
@@ -299,14 +327,14 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int sl, int loc
     }
     if (!want_wave) return ZERO;
     if (not_finite(un)) return 1e30f;
-    const float* D = sm + F_D * L::BOX;
+    const float* D = sm + L::off(F_D);
     const float d_left = D[b - S], d_right = D[b];
     const float dup = from_left ? d_left : d_right;
     if (dup <= P.h_cfl) return ZERO;
     // the plan shares of the face's two cells: from the image, or (a strip) from global memory at native index k
     float om_l, om_r;
     if constexpr (L::OM) {
-        const float* OM = sm + F_OM * L::BOX;
+        const float* OM = sm + L::off(F_OM);
         om_l = OM[b - S];
         om_r = OM[b];
     } else {
@@ -497,10 +525,11 @@ void launch_probe(const StepArgs& A, int t, float dt, float* out, cudaStream_t s
 
 // The strip forms of the face pass: the same faces, a strip of H rows of a tile at a time (H = 16: halves, H = 8:
 // quarters). A unit of work is one strip of a tile of the work list (32 / H units a tile); a CTA of 16 H threads (H / 2
-// warps, two rows a warp) stages the strip with TMA as eight 40 x (H + 4) boxes, its momenta as 32 x H boxes and its
-// twelve static face scalars as bulk copies: 54 KB for 16 rows, so that four CTAs share a SM, 30 KB for 8 rows, seven.
-// While one CTA waits for its copies the others compute (the tile form's two CTAs of 109 KB leave a SM idle whenever
-// both wait). The plan shares, wanted on refresh steps only, are read from
+// warps, two rows a warp) stages the strip with TMA as eight 40-column boxes of the rows each state field is read at
+// (StripImage), its momenta as 32 x H boxes and its twelve static face scalars as bulk copies: 51 KB for 16 rows, so
+// that four CTAs share a SM, 27 KB for 8 rows, eight (with 64 registers a thread). While one CTA waits for its copies
+// the others compute (the tile form's two CTAs of 109 KB leave a SM idle whenever both wait). The plan shares, wanted
+// on refresh steps only, are read from
 // global memory. A face's arithmetic is the tile form's, bit for bit. On refresh steps each strip's wave maximum goes
 // to its tile's entry and its run's maximum by integer atomic maxima on the float bits.
 template <int H, bool ON>
@@ -511,7 +540,7 @@ __global__ void __launch_bounds__(StripImage<H>::THREADS, StripImage<H>::CTAS)
     const StripMaps& SM_ = H == 16 ? M.s16 : M.s8;
     extern __shared__ __align__(128) float sm[];
     __shared__ __align__(8) uint64_t bar;
-    __shared__ float red[32];
+    __shared__ float red[L::THREADS / 32];
     __shared__ float rowc[2 * 64 + 1];
     Ctl* ctl = A.ctl;
     if (!(ctl->any & ANY_RUN)) return;
@@ -551,18 +580,19 @@ __global__ void __launch_bounds__(StripImage<H>::THREADS, StripImage<H>::CTAS)
         const int ts = table_of(A, t);
         if (tid == 0) {
             fence_proxy_async();
-            mbar_expect_tx(&bar, (uint32_t)L::SMEM);
-            const int x0 = ti * TILE + GX - 4, y0 = tj * TILE + GY + row0 - 2;
-            tma_load_2d(sm + F_D * L::BOX, &SM_.d, x0, y0, &bar);
-            tma_load_2d(sm + F_H * L::BOX, &SM_.h[p], x0, y0, &bar);
-            tma_load_2d(sm + F_U * L::BOX, &SM_.u[p], x0, y0, &bar);
-            tma_load_2d(sm + F_V * L::BOX, &SM_.v[p], x0, y0, &bar);
-            tma_load_2d(sm + F_QX * L::BOX, &SM_.qx, x0, y0, &bar);
-            tma_load_2d(sm + F_QY * L::BOX, &SM_.qy, x0, y0, &bar);
-            tma_load_2d(sm + L::ZCX * L::BOX, &SM_.zcx, x0, y0, &bar);
-            tma_load_2d(sm + L::ZCY * L::BOX, &SM_.zcy, x0, y0, &bar);
-            tma_load_2d(sm + L::M, &SM_.mx[p], x0 + 4, y0 + 2, &bar);
-            tma_load_2d(sm + L::M + L::S, &SM_.my[p], x0 + 4, y0 + 2, &bar);
+            mbar_expect_tx(&bar, (uint32_t)L::BYTES);
+            // each box from its first row (the strip's row 0 is y)
+            const int x0 = ti * TILE + GX - 4, y = tj * TILE + GY + row0;
+            tma_load_2d(sm + L::S_U, &SM_.u[p], x0, y - 2, &bar);
+            tma_load_2d(sm + L::S_V, &SM_.v[p], x0, y - 2, &bar);
+            tma_load_2d(sm + L::S_D, &SM_.d, x0, y - 1, &bar);
+            tma_load_2d(sm + L::S_H, &SM_.h[p], x0, y - 1, &bar);
+            tma_load_2d(sm + L::S_QX, &SM_.qx, x0, y - 1, &bar);
+            tma_load_2d(sm + L::S_QY, &SM_.qy, x0, y - 1, &bar);
+            tma_load_2d(sm + L::S_ZCX, &SM_.zcx, x0, y, &bar);
+            tma_load_2d(sm + L::S_ZCY, &SM_.zcy, x0, y - 1, &bar);
+            tma_load_2d(sm + L::M, &SM_.mx[p], x0 + 4, y, &bar);
+            tma_load_2d(sm + L::M + L::S, &SM_.my[p], x0 + 4, y, &bar);
             for (int f = 0; f < 12; ++f)
                 bulk_load(sm + L::ST + f * L::S, statics[f] + (size_t)ts * TILE2 + row0 * TILE, L::S * 4, &bar);
         }

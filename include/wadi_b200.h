@@ -362,7 +362,7 @@ int32_t w2b_build_tables_noalloc(const W2BTableIn* in, const W2BTableOut* out, v
  * strip forms), each timed with CUDA events from the end of the launch before it (the host's clock read between graphs
  * included) per loop step that ran; after three launches each the fastest is kept for the handle's life, the default
  * unless another is more than 2 % faster. The strip forms of the face pass take strips of 16 rows of a tile (CTAs of
- * 256 threads and 54 KB, four a SM) or of 8 rows (128 threads and 30 KB, seven a SM): the same faces bit for bit.
+ * 256 threads and 51 KB, four a SM) or of 8 rows (128 threads and 27 KB, eight a SM): the same faces bit for bit.
  * w2b_loop_tuning(h, 1, ...) starts tuning again; w2b_loop_tuning(h, tune, f, u, s) with tune 0, 2 or 3 fixes a
  * configuration with the tile form, the 16-row or the 8-row strips (1 <= f <= the form's resident CTAs a SM, 1 <= u <=
  * the update pass's, 1 <= s <= 64), W2B_EINVAL outside that. w2b_loop_config(h, out) fills out[9]: faces CTAs a SM,

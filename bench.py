@@ -38,12 +38,12 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-# Algorithmic bytes per cell-step. The whole step (the fused form): 44 B of state read, 40 B written, 60 B of static
-# scalars, 40 B of table values, 10 B of envelope (5 arrays read and written every 4 steps). The face pass alone:
-# d h u v mx my qx qy read (32 B) + om on refresh steps (4 B / 8), zcx zcy (8 B), 12 face scalars (48 B), two table
-# quads (32 B); u v mx my qx qy written (24 B).
-ALG_STEP = 194.0
-ALG_FACES = 32.0 + 0.5 + 8.0 + 48.0 + 32.0 + 24.0
+# Algorithmic bytes per cell-step. The whole step: 40 B of state read, 32 B written, 60 B of static scalars, 40 B of
+# table values, 10 B of envelope (5 arrays read and written every 4 steps). The face pass alone: d h u v qx qy and the
+# last step's mean depth read (28 B; the face momenta are formed from it and the velocities, not stored) + om on
+# refresh steps (4 B / 8), zcx zcy (8 B), 12 face scalars (48 B), two table quads (32 B); u v qx qy written (16 B).
+ALG_STEP = 182.0
+ALG_FACES = 28.0 + 0.5 + 8.0 + 48.0 + 32.0 + 16.0
 FALLBACK_HBM_GBS = 6650.0
 # DRAM bytes a tile cell of the face pass (dram__bytes_read.sum + dram__bytes_write.sum of one launch, divided by the
 # launch's tile cells), from an ncu capture of faces_kernel on configuration 3's catchment at 1024 x 1024 cells

@@ -212,12 +212,24 @@ int32_t w2b_wet_flags(void* handle, int32_t* out, void* stream);
 /* Replaces refresh_plan (wadi2d/solver/gpu/backend.py:139-143): tiles is a device array. */
 int32_t w2b_refresh_plan(void* handle, const int32_t* tiles, int32_t n, void* stream);
 
-/* Current device pointer of a field (ping-pong pairs resolve to their current half). */
+/* Current device pointer of a field (ping-pong pairs resolve to their current half). The face momenta (MX, MY) are
+ * not kept in their arrays while the library steps: a step's momentum is abar * u, with abar from the mean depths the
+ * step started from, so the next step forms it from the other half of the mean depth pair and the face velocity
+ * instead of reading it (12 bytes a cell less HBM traffic a step, the same bits). Before reading or writing U, V, MX,
+ * MY (or their other halves) through this pointer, call w2b_sync_momentum on the stream that will access them; the
+ * next step then starts from the arrays, written or not. MX1 and MY1 (the other halves) hold nothing between steps. */
 int32_t w2b_field_ptr(void* handle, int32_t field, float** out);
+
+/* The face momenta into their arrays (the current half of every run) and a record that the next step starts from
+ * them (no work if they are there already). No counterpart in the reference, which stores the momenta every step.
+ * In a batch, a momentum written for a run that does not step at the next loop step is formed from the state again
+ * after it. */
+int32_t w2b_sync_momentum(void* handle, void* stream);
 
 /* Replaces get_field / set_field (wadi2d/solver/gpu/backend.py:121-125). layout REF_TILE or NATIVE; host != 0 means
  * the other pointer is host memory (pinned for an asynchronous copy). REF_TILE writes own cells only: halo entries
- * of the reference layout are copies and are read back from their owners. */
+ * of the reference layout are copies and are read back from their owners. Both call w2b_sync_momentum first for U,
+ * V, MX, MY and their other halves. */
 int32_t w2b_get_field(void* handle, int32_t field, float* dst, int32_t layout, int32_t host, void* stream);
 int32_t w2b_set_field(void* handle, int32_t field, const float* src, int32_t layout, int32_t host, void* stream);
 

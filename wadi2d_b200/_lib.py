@@ -99,6 +99,7 @@ _SIGNATURES = {
     "w2b_wet_flags": [c_vp, c_vp, c_vp],
     "w2b_refresh_plan": [c_vp, c_vp, c_i32, c_vp],
     "w2b_field_ptr": [c_vp, c_i32, ctypes.POINTER(c_vp)],
+    "w2b_sync_momentum": [c_vp, c_vp],
     "w2b_get_field": [c_vp, c_i32, c_vp, c_i32, c_i32, c_vp],
     "w2b_set_field": [c_vp, c_i32, c_vp, c_i32, c_i32, c_vp],
     "w2b_maxima": [c_vp, c_f32, c_f32, c_f32, c_vp],

@@ -127,6 +127,7 @@ class TileFlags:
 STATE = ("h", "d", "u", "v", "mx", "my", "qx", "qy", "u1", "v1", "mx1", "my1", "qx1", "qy1", "src", "res", "om",
          "zcx", "zcy")  # fmt: skip
 ENVELOPE = ("depth", "mean_depth", "speed", "hazard", "arrival")
+MOMENTUM_FIELDS = ("u", "v", "mx", "my", "u1", "v1", "mx1", "my1")  # read or written only with the momenta in place
 
 
 class B200Backend:
@@ -274,7 +275,10 @@ class B200Backend:
         return self.torch.cuda.current_stream(self.device).cuda_stream
 
     def native(self, name: str):
-        """The current device tensor of a field, NATIVE layout."""
+        """The current device tensor of a field, NATIVE layout (for the velocities and momenta, with the momenta put in
+        their arrays first: w2b_sync_momentum)."""
+        if name in MOMENTUM_FIELDS:
+            self.sync_momentum()
         p = ctypes.c_void_p()
         _lib.call("w2b_field_ptr", self.handle, _lib.FIELD_ID[name], ctypes.byref(p))
         for key in ("h", "u", "v", "mx", "my"):
@@ -284,6 +288,11 @@ class B200Backend:
                     return pair[half]
         key = name
         return self._t[key]
+
+    def sync_momentum(self) -> None:
+        """The face momenta into their arrays, on the current stream, before the state is read or written directly
+        (the steps form them from the mean depths and face velocities instead of storing them)."""
+        _lib.call("w2b_sync_momentum", self.handle, self._stream())
 
     def __getattr__(self, name: str):
         if name in STATE:

@@ -489,6 +489,8 @@ class Batch:
         b = self.backend
         b.synchronize()
         if name in ("h", "u", "v", "mx", "my"):
+            if name in ("u", "v", "mx", "my"):
+                b.sync_momentum()
             t = b._t[name][int(self.halves()[r])]
         elif name in ("d", "qx", "qy", "qx1", "qy1", "res", "src", "om", "zcx", "zcy"):
             t = b._t[name]

@@ -3,6 +3,7 @@
 // The handle binds caller-owned device buffers; the only memory it allocates is its own host record and the CUDA
 // graphs of the device loop. Ping-pong pairs (h, u, v, mx, my) are resolved through the handle's parity, which
 // flips after every step: the reference swaps its arrays the same way (wadi2d/solver/gpu/backend.py:185-188).
+#include <cstddef>
 #include <cstdio>
 #include <cstring>
 #include <new>
@@ -54,6 +55,7 @@ static const Passes& passes(const W2BParams& P) { return P.arith == W2B_ARITH_FA
 
 void launch_cbrt_check(uint32_t first, uint32_t count, unsigned long long* out, cudaStream_t s);
 void launch_wait_check(uint32_t polls, long long* out, cudaStream_t s);
+void launch_momentum(const StepArgs& A, int sms, cudaStream_t s);
 __global__ void boundary_kernel(StepArgs A, int control);
 __global__ void envelope_kernel(StepArgs A);
 __global__ void control_kernel(StepArgs A);
@@ -513,6 +515,11 @@ int32_t w2b_create(const W2BGridDesc* grid, const W2BParams* params, const W2BBu
     H->nact = grid->ntiles - 1;
     H->nruns = grid->nruns;
     H->R = run_table(H->B.runs, H->nruns);
+    const int32_t stored = 1;  // the caller's momentum arrays hold the momenta the first step starts from
+    if (cudaMemcpy(&H->ctl()->m_stored, &stored, sizeof(stored), cudaMemcpyHostToDevice) != cudaSuccess) {
+        delete H;
+        return cuda_status(cudaGetLastError(), "w2b_create control block");
+    }
     if (H->nruns == 1 && cudaMemcpy(H->R.dx, &H->P.dx, sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
         delete H;
         return cuda_status(cudaGetLastError(), "w2b_create run table");
@@ -753,12 +760,29 @@ int32_t w2b_field_ptr(void* handle, int32_t field, float** out) {
     return W2B_OK;
 }
 
+// Fields whose reading or writing needs the momenta in their arrays: the momenta themselves, and the velocities they
+// are formed from (a velocity written afterwards must not change the momentum the next step starts from).
+static bool momentum_field(int f) {
+    return f == W2B_U || f == W2B_V || f == W2B_MX || f == W2B_MY || f == W2B_U1 || f == W2B_V1 || f == W2B_MX1 ||
+           f == W2B_MY1;
+}
+
+static int sync_momentum(Handle& H, cudaStream_t s) {
+    launch_momentum(make_args(H), H.sms, s);
+    CKL("w2b_sync_momentum");
+    return W2B_OK;
+}
+
 int32_t w2b_get_field(void* handle, int32_t field, float* dst, int32_t layout, int32_t host, void* stream) {
     if (!handle || !dst) return W2B_EINVAL;
     Handle* H = static_cast<Handle*>(handle);
     float* src = field_ptr(H, field);
     if (!src) return W2B_EINVAL;
     cudaStream_t s = (cudaStream_t)stream;
+    if (momentum_field(field)) {
+        const int st = sync_momentum(*H, s);
+        if (st != W2B_OK) return st;
+    }
     if (layout == W2B_LAYOUT_NATIVE) {
         CK(cudaMemcpyAsync(dst, src, sizeof(float) * H->L.ncells,
                            host ? cudaMemcpyDeviceToHost : cudaMemcpyDeviceToDevice, s));
@@ -782,6 +806,10 @@ int32_t w2b_set_field(void* handle, int32_t field, const float* src, int32_t lay
     float* dst = field_ptr(H, field);
     if (!dst) return W2B_EINVAL;
     cudaStream_t s = (cudaStream_t)stream;
+    if (momentum_field(field)) {
+        const int st = sync_momentum(*H, s);
+        if (st != W2B_OK) return st;
+    }
     if (layout == W2B_LAYOUT_NATIVE) {
         CK(cudaMemcpyAsync(dst, src, sizeof(float) * H->L.ncells,
                            host ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToDevice, s));
@@ -800,6 +828,11 @@ int32_t w2b_set_field(void* handle, int32_t field, const float* src, int32_t lay
     }
     if (host) CK(cudaStreamSynchronize(s));
     return W2B_OK;
+}
+
+int32_t w2b_sync_momentum(void* handle, void* stream) {
+    if (!handle) return W2B_EINVAL;
+    return sync_momentum(*static_cast<Handle*>(handle), (cudaStream_t)stream);
 }
 
 int32_t w2b_maxima(void* handle, float t, float arrive, float deep, void* stream) {
@@ -897,7 +930,7 @@ static int advance_runs(Handle* H, const W2BStepper* cfg, const double* t_end, i
         rd[r] = clocks[r].refresh_due;
     }
     const RunTab& R = H->R;
-    CK(cudaMemcpyAsync(H->ctl(), &c, sizeof(Ctl), cudaMemcpyHostToDevice, s));
+    CK(cudaMemcpyAsync(H->ctl(), &c, offsetof(Ctl, m_stored), cudaMemcpyHostToDevice, s));  // the flag stays
     CK(cudaMemcpyAsync(R.t, t.data(), 8 * n, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(R.dt, dt.data(), 8 * n, cudaMemcpyHostToDevice, s));
     CK(cudaMemcpyAsync(R.t_end, te.data(), 8 * n, cudaMemcpyHostToDevice, s));

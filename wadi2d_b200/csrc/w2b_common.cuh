@@ -31,6 +31,11 @@ struct Ctl {
     int32_t dt_every, active_every, adaptive, max_every;
     float arrive, deep;
     double cfl, wave_floor, dt_max, dt_min;
+    // 1 while the momentum arrays hold the face momenta (set at creation and by w2b_sync_momentum), 0 once a face pass
+    // has stepped: the face pass then forms each face's momentum from the state instead of reading it (the momentum
+    // after a step is abar * u with abar from the mean depths the step started from, which are still the other half
+    // of the ping-pong pair). Last member: the device loop's settings overwrite the block up to it.
+    int32_t m_stored;
 };
 static_assert(sizeof(Ctl) <= W2B_CTL_BYTES, "control block too large");
 

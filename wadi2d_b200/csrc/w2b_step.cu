@@ -48,6 +48,7 @@ constexpr int FACES_THREADS = 512;
 // static face scalar's (and of a momentum's) array in the image: 1,024 floats for a tile, 32 H for a strip.
 struct TileImage {
     static constexpr int M = SM_M, ST = SM_ST, S = TILE2;
+    static constexpr int HO = SM_M;  // the last step's mean depth box (40 x 36), in the momenta's place
     static constexpr bool OM = true;
     __host__ __device__ static constexpr int off(int f) { return f * BOX; }
 };
@@ -65,11 +66,16 @@ struct StripImage {
     static constexpr int S_QY = S_QX + pad32(BOXW * R_1), S_ZCX = S_QY + pad32(BOXW * R_QY);
     static constexpr int S_ZCY = S_ZCX + pad32(BOXW * R_ZCX), S_END = S_ZCY + pad32(BOXW * R_1);
     static constexpr int M = S_END, ST = S_END + 2 * TILE * H, S = TILE * H;
+    // the last step's mean depth box, in the momenta's place: the rows of the mean depth's box, BOXW * (H + 1) <=
+    // 2 TILE H floats
+    static constexpr int HO = M - BOXW;
     static constexpr bool OM = false;
     static constexpr int FLOATS = ST + 12 * S;
     static constexpr int SMEM = FLOATS * 4;        // 51,840 bytes for 16 rows (four CTAs a SM), 27,264 for 8 (eight)
-    // the bytes the strip's copies bring (the regions without their padding)
+    // the bytes the strip's copies bring (the regions without their padding): with the momenta, or with the last
+    // step's mean depth in their place
     static constexpr int BYTES = 4 * (BOXW * (2 * R_UV + 4 * R_1 + R_QY + R_ZCX) + 14 * TILE * H);
+    static constexpr int BYTES_HO = BYTES - 4 * (2 * TILE * H - BOXW * R_1);
     static constexpr int THREADS = 16 * H;         // a warp two rows
     static constexpr int CTAS = H == 16 ? 4 : 8;   // resident CTAs a SM the launch bound plans for
     __host__ __device__ static constexpr int off(int f) {
@@ -85,6 +91,9 @@ struct StripImage {
 };
 static_assert(StripImage<8>::SMEM == 27264 && StripImage<16>::SMEM == 51840, "strip image sizes");
 static_assert(StripImage<8>::off(F_D) >= 0 && StripImage<8>::off(F_ZCX) >= 0, "strip offsets");
+static_assert(BOXW * StripImage<8>::R_1 <= 2 * TILE * 8 && BOXW * StripImage<16>::R_1 <= 2 * TILE * 16 &&
+                  BOX <= 2 * TILE2,
+              "the last step's mean depth box fits the momenta's place");
 
 // What the first part of a face hands to the rest: the row's quad (its load is issued in part A and consumed after
 // the table-free momentum terms), the face depth, and the table row with the upwind choice, the live flag and the
@@ -155,11 +164,14 @@ __device__ __forceinline__ void face_a(const float* sm, int b, int sl, int local
 
 // Parts B and C: the momentum terms (faces.cu:50-100, table-free), then the lookup, section, friction, crest cap,
 // outputs and wave speed (faces.cu:43-44, :52-63, :102-145). Returns the wave speed.
+// mst: the face's momentum is the image's stored one (Ctl::m_stored), else it is formed from the last step's mean
+// depths (the image's HO box) and the face velocity, as the step that wrote the velocity formed it. The new momentum
+// is not written: the next step forms it the same way.
 // PROBE: write the face's new velocity to probe_un[local] and nothing of the state (the step-limiter probe).
 template <int AX, bool PROBE = false, bool ON = false, class L = TileImage>
 __device__ __forceinline__ float face_bc(const float* sm, int b, int sl, int local, int k, const StepArgs& A, int t,
                                          const FaceA& F, float dt, float dx, int want_wave, const float* rowc, int p,
-                                         float* probe_un = nullptr) {
+                                         int mst, float* probe_un = nullptr) {
     constexpr int S = AX == 0 ? 1 : BOXW;
     constexpr int PP = AX == 0 ? BOXW : 1;
     const W2BParams& P = A.P;
@@ -168,7 +180,6 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int sl, int loc
             probe_un[local] = 0.0f;
         } else {
             A.uu[AX][1 - p][k] = 0.0f;
-            A.mm[AX][1 - p][k] = 0.0f;
             A.q1[AX][k] = 0.0f;
         }
         return 0.0f;
@@ -229,19 +240,24 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int sl, int loc
     // [4] momentum and pressure (the fast build multiplies by one reciprocal of the span, which the compiler hoists
     // out of the tile's loop)
     const float abar = HALF * (h_l + h_r) * dx;
+    // the face's momentum (the last step's abar * u, rounded once as that step rounded it)
+    const float* HO = sm + L::HO;
+    auto momentum = [&]() {
+        return mst ? sm[L::M + AX * L::S + sl] : __fmul_rn(HALF * (HO[b - S] + HO[b]) * dx, uf);
+    };
 #ifdef W2B_FAST
     const float rspan = __fdividef(ONE, span);
     const float press = dt * P.g * d_eta * rspan;
     float us;
     if (abar > 1e-6f * dx)
-        us = qdiv(sm[L::M + AX * L::S + sl] - dt * flux * rspan, abar) - press;
+        us = qdiv(momentum() - dt * flux * rspan, abar) - press;
     else
         us = uf - press;
 #else
     const float press = qdiv(dt * P.g * d_eta, span);
     float us;
     if (abar > 1e-6f * dx)
-        us = qdiv(sm[L::M + AX * L::S + sl] - qdiv(dt * flux, span), abar) - press;
+        us = qdiv(momentum() - qdiv(dt * flux, span), abar) - press;
     else
         us = uf - press;
 #endif
@@ -322,7 +338,6 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int sl, int loc
         probe_un[local] = un;
     } else {
         A.uu[AX][1 - p][k] = un;
-        A.mm[AX][1 - p][k] = abar * un;
         A.q1[AX][k] = qn;
     }
     if (!want_wave) return ZERO;
@@ -371,7 +386,8 @@ __device__ __forceinline__ float block_max(float v, float* red) {
 
 // The face pass: both own faces of every cell of the tiles of the work list (wadi2d/solver/gpu/kernels/faces.cu:
 // 148-175). Each CTA (16 warps, a warp a tile row, two rows a warp; two CTAs a SM) stages a tile with TMA: nine
-// 40 x 36 state boxes, the two momenta, and the tile's twelve static face scalars as bulk copies; on refresh steps
+// 40 x 36 state boxes, the two momenta (or, once a face pass has stepped, the last step's mean depth box they are
+// formed from), and the tile's twelve static face scalars as bulk copies; on refresh steps
 // the tile's wave maximum goes to its run's maximum (an integer atomic max on the float bits). p is the parity of
 // the run's ping-pong halves.
 template <bool ON>
@@ -383,6 +399,7 @@ __global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_co
     Ctl* ctl = A.ctl;
     if (!(ctl->any & ANY_RUN)) return;
     const int nwork = ctl->nwork;
+    const int mst = ctl->m_stored;
     const int tid = threadIdx.x;
     if (tid == 0) {
         mbar_init(&bar, 1);
@@ -417,7 +434,7 @@ __global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_co
         const int ts = table_of(A, t);
         if (tid == 0) {
             fence_proxy_async();
-            mbar_expect_tx(&bar, (uint32_t)((NBOX - (want_wave ? 0 : 1)) * BOX + 14 * TILE2) * 4u);
+            mbar_expect_tx(&bar, (uint32_t)((NBOX - (want_wave ? 0 : 1)) * BOX + (mst ? 14 * TILE2 : BOX + 12 * TILE2)) * 4u);
             const int x0 = ti * TILE + GX - 4, y0 = tj * TILE + GY - 2;
             tma_load_2d(sm + F_D * BOX, &M.d, x0, y0, &bar);
             tma_load_2d(sm + F_H * BOX, &M.h[p], x0, y0, &bar);
@@ -428,8 +445,12 @@ __global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_co
             if (want_wave) tma_load_2d(sm + F_OM * BOX, &M.om, x0, y0, &bar);
             tma_load_2d(sm + F_ZCX * BOX, &M.zcx, x0, y0, &bar);
             tma_load_2d(sm + F_ZCY * BOX, &M.zcy, x0, y0, &bar);
-            tma_load_2d(sm + SM_M, &M.mx[p], x0 + 4, y0 + 2, &bar);
-            tma_load_2d(sm + SM_M + TILE2, &M.my[p], x0 + 4, y0 + 2, &bar);
+            if (mst) {
+                tma_load_2d(sm + SM_M, &M.mx[p], x0 + 4, y0 + 2, &bar);
+                tma_load_2d(sm + SM_M + TILE2, &M.my[p], x0 + 4, y0 + 2, &bar);
+            } else {
+                tma_load_2d(sm + TileImage::HO, &M.h[1 - p], x0, y0, &bar);
+            }
             for (int f = 0; f < 12; ++f) bulk_load(sm + SM_ST + f * TILE2, statics[f] + (size_t)ts * TILE2, TILE2 * 4, &bar);
         }
         const bool ok = mbar_wait(&bar, phase);
@@ -451,8 +472,8 @@ __global__ void __launch_bounds__(FACES_THREADS, 2) faces_kernel(const __grid_co
             FaceA fx, fy;
             face_a<0, ON>(sm, b, local, local, A, ts, fx);
             face_a<1, ON>(sm, b, local, local, A, ts, fy);
-            const float wx = face_bc<0, false, ON>(sm, b, local, local, k, A, ts, fx, dt, dx, want_wave, rowc, p);
-            const float wy = face_bc<1, false, ON>(sm, b, local, local, k, A, ts, fy, dt, dx, want_wave, rowc, p);
+            const float wx = face_bc<0, false, ON>(sm, b, local, local, k, A, ts, fx, dt, dx, want_wave, rowc, p, mst);
+            const float wy = face_bc<1, false, ON>(sm, b, local, local, k, A, ts, fy, dt, dx, want_wave, rowc, p, mst);
             wmax = fmax32(wmax, fmax32(wx, wy));
         }
         if (want_wave) {
@@ -482,17 +503,21 @@ __global__ void __launch_bounds__(1024) probe_kernel(StepArgs A, int t, float dt
     const float dx = A.R.dx[run];
     const int tj = A.tiles[2 * t], ti = A.tiles[2 * t + 1];
     const int x0 = ti * TILE + GX - 4, y0 = tj * TILE + GY - 2;
+    const int mst = A.ctl->m_stored;
     const float* boxes[NBOX] = {A.d, A.hh[p], A.uu[0][p], A.uu[1][p], A.q[0], A.q[1], A.om, A.zc[0], A.zc[1]};
     for (int idx = tid; idx < BOX; idx += blockDim.x) {
         const size_t k = (size_t)(y0 + idx / BOXW) * A.px + x0 + idx % BOXW;
         for (int f = 0; f < NBOX; ++f) sm[f * BOX + idx] = boxes[f][k];
+        if (!mst) sm[TileImage::HO + idx] = A.hh[1 - p][k];
     }
     const float* statics[12] = {A.fl[0], A.fr[0], A.gl[0], A.gr[0], A.ef[0], A.cw[0],
                                 A.fl[1], A.fr[1], A.gl[1], A.gr[1], A.ef[1], A.cw[1]};
     for (int idx = tid; idx < TILE2; idx += blockDim.x) {
         const size_t k = (size_t)(tj * TILE + GY + idx / TILE) * A.px + ti * TILE + GX + idx % TILE;
-        sm[SM_M + idx] = A.mm[0][p][k];
-        sm[SM_M + TILE2 + idx] = A.mm[1][p][k];
+        if (mst) {
+            sm[SM_M + idx] = A.mm[0][p][k];
+            sm[SM_M + TILE2 + idx] = A.mm[1][p][k];
+        }
         for (int f = 0; f < 12; ++f) sm[SM_ST + f * TILE2 + idx] = statics[f][(size_t)table_of(A, t) * TILE2 + idx];
     }
     if (tid < A.rows - 1) {
@@ -515,8 +540,8 @@ __global__ void __launch_bounds__(1024) probe_kernel(StepArgs A, int t, float dt
     const int ts = table_of(A, t);
     face_a<0>(sm, b, local, local, A, ts, fx);
     face_a<1>(sm, b, local, local, A, ts, fy);
-    out[local] = face_bc<0, true>(sm, b, local, local, k, A, ts, fx, dt, dx, 1, rowc, p, out + 2 * TILE2);
-    out[TILE2 + local] = face_bc<1, true>(sm, b, local, local, k, A, ts, fy, dt, dx, 1, rowc, p, out + 3 * TILE2);
+    out[local] = face_bc<0, true>(sm, b, local, local, k, A, ts, fx, dt, dx, 1, rowc, p, mst, out + 2 * TILE2);
+    out[TILE2 + local] = face_bc<1, true>(sm, b, local, local, k, A, ts, fy, dt, dx, 1, rowc, p, mst, out + 3 * TILE2);
 }
 
 void launch_probe(const StepArgs& A, int t, float dt, float* out, cudaStream_t s) {
@@ -545,6 +570,7 @@ __global__ void __launch_bounds__(StripImage<H>::THREADS, StripImage<H>::CTAS)
     Ctl* ctl = A.ctl;
     if (!(ctl->any & ANY_RUN)) return;
     const int nunits = PER * ctl->nwork;
+    const int mst = ctl->m_stored;
     const int tid = threadIdx.x;
     if (tid == 0) {
         mbar_init(&bar, 1);
@@ -580,7 +606,7 @@ __global__ void __launch_bounds__(StripImage<H>::THREADS, StripImage<H>::CTAS)
         const int ts = table_of(A, t);
         if (tid == 0) {
             fence_proxy_async();
-            mbar_expect_tx(&bar, (uint32_t)L::BYTES);
+            mbar_expect_tx(&bar, (uint32_t)(mst ? L::BYTES : L::BYTES_HO));
             // each box from its first row (the strip's row 0 is y)
             const int x0 = ti * TILE + GX - 4, y = tj * TILE + GY + row0;
             tma_load_2d(sm + L::S_U, &SM_.u[p], x0, y - 2, &bar);
@@ -591,8 +617,12 @@ __global__ void __launch_bounds__(StripImage<H>::THREADS, StripImage<H>::CTAS)
             tma_load_2d(sm + L::S_QY, &SM_.qy, x0, y - 1, &bar);
             tma_load_2d(sm + L::S_ZCX, &SM_.zcx, x0, y, &bar);
             tma_load_2d(sm + L::S_ZCY, &SM_.zcy, x0, y - 1, &bar);
-            tma_load_2d(sm + L::M, &SM_.mx[p], x0 + 4, y, &bar);
-            tma_load_2d(sm + L::M + L::S, &SM_.my[p], x0 + 4, y, &bar);
+            if (mst) {
+                tma_load_2d(sm + L::M, &SM_.mx[p], x0 + 4, y, &bar);
+                tma_load_2d(sm + L::M + L::S, &SM_.my[p], x0 + 4, y, &bar);
+            } else {
+                tma_load_2d(sm + L::M, &SM_.h[1 - p], x0, y - 1, &bar);  // the mean depth box's rows
+            }
             for (int f = 0; f < 12; ++f)
                 bulk_load(sm + L::ST + f * L::S, statics[f] + (size_t)ts * TILE2 + row0 * TILE, L::S * 4, &bar);
         }
@@ -617,9 +647,9 @@ __global__ void __launch_bounds__(StripImage<H>::THREADS, StripImage<H>::CTAS)
             face_a<0, ON, L>(sm, b, sl, local, A, ts, fx);
             face_a<1, ON, L>(sm, b, sl, local, A, ts, fy);
             const float wx = face_bc<0, false, ON, L>(sm, b, sl, local, k, A, ts, fx, dt, dx, want_wave, rowc,
-                                                               p);
+                                                               p, mst);
             const float wy = face_bc<1, false, ON, L>(sm, b, sl, local, k, A, ts, fy, dt, dx, want_wave, rowc,
-                                                               p);
+                                                               p, mst);
             wmax = fmax32(wmax, fmax32(wx, wy));
         }
         if (want_wave) {
@@ -752,6 +782,8 @@ __global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_con
     const int nwork = ctl->nwork;
     const int px = A.px;
     const int tid = threadIdx.y * blockDim.x + threadIdx.x;
+    // the face pass before this one has stepped: from now on the momenta are formed from the state (Ctl::m_stored)
+    if (blockIdx.x == 0 && tid == 0) ctl->m_stored = 0;
     const int rows = A.rows, last = rows - 1;
     if (tid == 0) {
         mbar_init(&bar, 1);
@@ -937,6 +969,36 @@ __global__ void wait_check_kernel(uint32_t polls, long long* out) {
 }
 
 void launch_wait_check(uint32_t polls, long long* out, cudaStream_t s) { wait_check_kernel<<<1, 32, 0, s>>>(polls, out); }
+
+// ------------------------------------------------------------------ face momenta
+
+// The face momenta into their arrays (each run's current half), as the face pass forms them once a face pass has
+// stepped: the last step's abar * u, abar from the other half of the mean depth pair (the depths that step started
+// from), rounded once. Every own face of every tile; nothing when the arrays already hold the momenta
+// (Ctl::m_stored), so it may run before any read or write of the state. momentum_mark_kernel, after it, records that
+// they do.
+__global__ void momentum_kernel(StepArgs A) {
+    if (A.ctl->m_stored) return;
+    const long long n = (long long)(A.ntiles - 1) * TILE2;
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        const int t = 1 + (int)(i / TILE2), c = (int)(i % TILE2);  // tile 0 is the void tile
+        const int run = A.tile_run[t];
+        const int p = A.R.parity[run];
+        const float dx = A.R.dx[run];
+        const int tj = A.tiles[2 * t], ti = A.tiles[2 * t + 1];
+        const size_t k = (size_t)(tj * TILE + GY + c / TILE) * A.px + ti * TILE + GX + c % TILE;
+        const float* ho = A.hh[1 - p];
+        A.mm[0][p][k] = __fmul_rn(0.5f * (ho[k - 1] + ho[k]) * dx, A.uu[0][p][k]);
+        A.mm[1][p][k] = __fmul_rn(0.5f * (ho[k - A.px] + ho[k]) * dx, A.uu[1][p][k]);
+    }
+}
+
+__global__ void momentum_mark_kernel(Ctl* ctl) { ctl->m_stored = 1; }
+
+void launch_momentum(const StepArgs& A, int sms, cudaStream_t s) {
+    momentum_kernel<<<sms * 4, 256, 0, s>>>(A);
+    momentum_mark_kernel<<<1, 1, 0, s>>>(A.ctl);
+}
 
 // ------------------------------------------------------------------ envelope pass
 

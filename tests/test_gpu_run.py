@@ -199,3 +199,35 @@ def test_fp64_level_in_the_near_dry_interval():
     sd = np.sqrt(h.astype(np.float64) / np.where(hc > 0, hc, 1.0).astype(np.float64)) * float(last)
     want = (t0 + sd * (t1 - t0)).astype(np.float32)
     assert np.array_equal(d_on[first], want[first])
+
+
+def test_staged_source_windows_equal_the_synchronous_upload():
+    """Each window's rates staged by SourceStager (uploaded on a side stream while the window before steps, then put
+    in place by a device copy) give the run that a synchronous upload of the same rates gives, bit for bit; the rates
+    differ from window to window, so a copy that landed late or early would show."""
+    from wadi2d_b200 import _lib
+    from wadi2d_b200.run import SourceStager
+
+    w, og, g, tab = c1(64)
+    a, b, c = (Model(GridTables.from_dict(g, tab), Numerics(arithmetic="fast")) for _ in range(3))
+    for m in (a, b):
+        m.stepper.adaptive_active = False
+        m.set_depth(np.where(g.mask, 0.02, 0.0))
+    rng = np.random.default_rng(9)
+    natives = []
+    for k in range(6):
+        c.set_source(np.where(g.mask, rng.random(g.shape) * 2e-5 * (k + 1), 0.0))
+        natives.append(c.backend.native("src").cpu().pin_memory())
+    stager = SourceStager(b)
+    stager.stage(natives[0])
+    for k, rates in enumerate(natives):
+        _lib.call("w2b_set_field", a.backend.handle, _lib.FIELD_ID["src"], rates.data_ptr(), _lib.LAYOUT_NATIVE, 1,
+                  a.backend._stream())  # fmt: skip
+        a.run(30.0 * (k + 1))
+        stager.commit()
+        if k + 1 < len(natives):
+            stager.stage(natives[k + 1])
+        b.run(30.0 * (k + 1))
+    assert a.stepper.nsteps == b.stepper.nsteps > 6
+    for name in ("h", "d", "u", "v", "qx", "qy", "mx", "my", "src"):
+        assert np.array_equal(a.field(name), b.field(name)), name

@@ -6,7 +6,8 @@ Rain comes either from the host (``forcing.Forcing.rate``, the reference's form:
 uploaded each window) or from the device (``DeviceRain``: the same rate formed on the GPU from per-cell storm depth
 multipliers, which removes the per-window upload). Lumped inflows likewise: on the host (``Forcing`` with
 injections, the cells' levels read back from the device each window) or on the device (``DeviceInflow``: each
-hydrograph's window flow shared by the levels read in place, no read-back and no upload).
+hydrograph's window flow shared by the levels read in place, no read-back and no upload). A host that knows its next
+window's rates ahead can upload them while the current window steps (``SourceStager``).
 """
 
 from __future__ import annotations
@@ -130,6 +131,45 @@ class DeviceStorage:
         _lib.call("w2b_storage", b.handle, int(self.cells.numel()), self.cells.data_ptr(), self.partial.data_ptr(),
                   self.out.data_ptr(), b._stream())  # fmt: skip
         return float(self.out.item())
+
+
+class SourceStager:
+    """Double-buffered upload of the source field, for a host whose next window's rates are known before the current
+    window has stepped (rain read from a radar or forecast grid, a precomputed storm): ``stage`` copies the next
+    window's rates, NATIVE layout, from pinned host memory into a device buffer on a side stream and returns at once;
+    ``commit`` (at the window's start) makes the step's stream wait for that copy and puts the rates in place with a
+    device-to-device copy (w2b_set_field, about 20 us for 16.8 M cells). The host-to-device copy thus overlaps the
+    stepping of the window before. The host buffer must not change until the next ``commit`` has returned."""
+
+    def __init__(self, model) -> None:
+        b = model.backend
+        self.b, self.torch = b, b.torch
+        self.buf = self.torch.empty(b.native("src").numel(), dtype=self.torch.float32, device=b.device)
+        self.side = self.torch.cuda.Stream(device=b.device)
+        self.ready = self.torch.cuda.Event()
+        self.pending = False
+
+    def stage(self, rates) -> int:
+        """Start the copy of ``rates`` (a pinned host tensor of the NATIVE field's size); returns its bytes."""
+        if rates.numel() != self.buf.numel() or rates.dtype != self.torch.float32:
+            raise ValueError(f"stage: {rates.numel()} {rates.dtype} values for {self.buf.numel()} float32")
+        cur = self.torch.cuda.current_stream(self.b.device)
+        self.side.wait_stream(cur)  # the buffer's last commit has been copied out
+        with self.torch.cuda.stream(self.side):
+            self.buf.copy_(rates, non_blocking=True)
+        self.ready.record(self.side)
+        self.pending = True
+        return rates.numel() * 4
+
+    def commit(self) -> None:
+        """The staged rates into the source field, ordered on the current stream after their upload."""
+        if not self.pending:
+            raise RuntimeError("commit: nothing staged")
+        cur = self.torch.cuda.current_stream(self.b.device)
+        cur.wait_event(self.ready)
+        _lib.call("w2b_set_field", self.b.handle, _lib.FIELD_ID["src"], self.buf.data_ptr(), _lib.LAYOUT_NATIVE, 0,
+                  cur.cuda_stream)  # fmt: skip
+        self.pending = False
 
 
 @dataclass

@@ -954,6 +954,9 @@ def main() -> None:
     env_host = [torch.empty(a.shape, dtype=a.dtype).pin_memory() for a in maxima.arrays]  # the maps' host buffers
     win = 30.0
     h2d = d2h = 0
+    # the monitor's reads once before the timed region, as the steps are warmed: their kernels' first launches (about
+    # 20 ms, once a process) belong to a run's set-up, not to each of its thousands of windows
+    line.discharge(), tally.volume(), storage()
     torch.cuda.synchronize(dev)
     w0 = time.perf_counter()
     s0 = m.stepper.nsteps

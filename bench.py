@@ -45,11 +45,11 @@ sys.path.insert(0, str(ROOT))
 ALG_STEP = 182.0
 ALG_FACES = 28.0 + 0.5 + 8.0 + 48.0 + 32.0 + 16.0
 FALLBACK_HBM_GBS = 6650.0
-# DRAM bytes a tile cell of the face pass (dram__bytes_read.sum + dram__bytes_write.sum of one launch, divided by the
-# launch's tile cells), from an ncu capture of faces_kernel on configuration 3's catchment at 1024 x 1024 cells
-# (1,115,136 tile cells, beyond L2); the traffic grows with the tile cells a launch processes, so it scales to this
-# launch by them.
-FACES_DRAM_BYTES_PER_CELL = 178.6
+# DRAM bytes a tile cell of the face pass (dram__bytes_read.sum + dram__bytes_write.sum of two launches, divided by
+# their tile cells), from an ncu capture of fast::strips_kernel<8> (the form the tuner keeps) on configuration 3's
+# catchment at 1024 x 1024 cells (1,115,136 tile cells a launch, beyond L2): profiles/strips8_kernel_fast_config3_1024.md.
+# The traffic grows with the tile cells a launch processes, so it scales to this launch by them.
+FACES_DRAM_BYTES_PER_CELL = 166.6
 CPU_BLOCK_TILES = 32  # the CPU sample: a 32 x 32-tile block (1,044,484 active cells) from the middle of the grid
 
 

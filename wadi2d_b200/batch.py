@@ -383,6 +383,7 @@ class Batch:
         if self._push_idle:
             b._t["idle"].copy_(torch.as_tensor(st.idle, device=b.device))
             self._push_idle = False
+        st._dev_keep = st._dev_idle = None  # this loop keeps its own account of what the device holds
         cfg = _lib.Stepper(num.cfl, num.wave_floor, num.dt_max, num.dt_min, num.dt_every, num.active_every,
                            int(st.adaptive_active), int(max_every), arrive, deep)  # fmt: skip
         clocks = np.zeros(n, CLOCK)

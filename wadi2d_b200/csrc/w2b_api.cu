@@ -901,6 +901,23 @@ static void tune_sample(Handle& H, int c, long long live, float ms) {
         if (k != best) drop_graph(H, k);
 }
 
+// A single run's loop settings and clock, written by one thread from its arguments. A copy from the host would be
+// queued on a copy engine behind any large upload in flight on another stream (the next window's source, staged while
+// this window steps) and wait for it; kernel arguments travel with the launch. The stored-momenta flag stays.
+__global__ void advance_setup_kernel(Ctl c, double t, double dt, double t_end, long long nsteps, long long max_steps,
+                                     int32_t refresh_due, Ctl* ctl, RunTab R) {
+    c.m_stored = ctl->m_stored;
+    *ctl = c;
+    R.t[0] = t;
+    R.dt[0] = dt;
+    R.t_end[0] = t_end;
+    R.nsteps[0] = nsteps;
+    R.steps_run[0] = 0;
+    R.max_steps[0] = max_steps;
+    R.refresh_due[0] = refresh_due;
+    R.status[0] = 0;
+}
+
 // The device-resident loop. Steps run in chunks of a captured graph (the launch configuration's steps), every running
 // run advancing one of its own steps each graph step; after each chunk the host reads the runs' clocks once.
 static int advance_runs(Handle* H, const W2BStepper* cfg, const double* t_end, int64_t max_steps, W2BClock* clocks,
@@ -930,15 +947,20 @@ static int advance_runs(Handle* H, const W2BStepper* cfg, const double* t_end, i
         rd[r] = clocks[r].refresh_due;
     }
     const RunTab& R = H->R;
-    CK(cudaMemcpyAsync(H->ctl(), &c, offsetof(Ctl, m_stored), cudaMemcpyHostToDevice, s));  // the flag stays
-    CK(cudaMemcpyAsync(R.t, t.data(), 8 * n, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(R.dt, dt.data(), 8 * n, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(R.t_end, te.data(), 8 * n, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(R.nsteps, ns.data(), 8 * n, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(R.steps_run, zero.data(), 8 * n, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(R.max_steps, ms.data(), 8 * n, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(R.refresh_due, rd.data(), 4 * n, cudaMemcpyHostToDevice, s));
-    CK(cudaMemcpyAsync(R.status, st.data(), 4 * n, cudaMemcpyHostToDevice, s));
+    if (n == 1) {  // by kernel arguments: no host-to-device copy (see advance_setup_kernel)
+        advance_setup_kernel<<<1, 1, 0, s>>>(c, t[0], dt[0], te[0], ns[0], ms[0], rd[0], H->ctl(), R);
+        CKL("advance settings");
+    } else {
+        CK(cudaMemcpyAsync(H->ctl(), &c, offsetof(Ctl, m_stored), cudaMemcpyHostToDevice, s));  // the flag stays
+        CK(cudaMemcpyAsync(R.t, t.data(), 8 * n, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(R.dt, dt.data(), 8 * n, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(R.t_end, te.data(), 8 * n, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(R.nsteps, ns.data(), 8 * n, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(R.steps_run, zero.data(), 8 * n, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(R.max_steps, ms.data(), 8 * n, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(R.refresh_due, rd.data(), 4 * n, cudaMemcpyHostToDevice, s));
+        CK(cudaMemcpyAsync(R.status, st.data(), 4 * n, cudaMemcpyHostToDevice, s));
+    }
     activity_kernel<<<1, 1024, 0, s>>>(make_args(*H), 1);  // the work list of the runs that take a step
     prestep_kernel<<<1, 1024, 0, s>>>(make_args(*H));      // the first step's settings; each step sets the next's
     CKL("advance work list");

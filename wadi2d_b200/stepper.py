@@ -43,6 +43,11 @@ class Stepper:
         self.kick = None
         self.wake_rules: list[Callable[[np.ndarray], np.ndarray]] = []
         self.idle = np.zeros(self.grid.ntiles, np.int32)
+        # what the device's keep flags and idle counts hold, as far as this stepper knows (None: unknown); the device
+        # loop uploads them only when the host's copies differ, so that a window's advance issues no host-to-device
+        # copy of its own while the next window's source is uploaded (run.SourceStager)
+        self._dev_keep: np.ndarray | None = None
+        self._dev_idle: np.ndarray | None = None
 
     def pin(self, tiles: np.ndarray) -> None:
         """Tiles that must see every smallest step; the uniform step has no other kind."""
@@ -121,8 +126,12 @@ class Stepper:
         torch = b.torch
         if not self.adaptive_active and int(b.nact) != self.grid.ntiles - 1:
             b.set_active(np.arange(1, self.grid.ntiles, dtype=np.int32))
-        b._t["keep"].copy_(torch.as_tensor(self.keep_active.astype(np.int32), device=b.device))
-        b._t["idle"].copy_(torch.as_tensor(self.idle, device=b.device))
+        keep = self.keep_active.astype(np.int32)
+        if self._dev_keep is None or not np.array_equal(keep, self._dev_keep):
+            b._t["keep"].copy_(torch.as_tensor(keep, device=b.device))
+            self._dev_keep = keep
+        if self._dev_idle is None or not np.array_equal(self.idle, self._dev_idle):
+            b._t["idle"].copy_(torch.as_tensor(self.idle, device=b.device))
         num = self.num
         cfg = _lib.Stepper(num.cfl, num.wave_floor, num.dt_max, num.dt_min, num.dt_every, num.active_every,
                            int(self.adaptive_active), int(max_every), arrive, deep)  # fmt: skip
@@ -135,6 +144,7 @@ class Stepper:
         b.active_tiles = b._t["active"][:nact].cpu().numpy().astype(np.int32)
         b.nact = nact
         self.idle[:] = b._t["idle"].cpu().numpy()
+        self._dev_idle = self.idle.copy()
         if status == _lib.ENONFINITE:
             raise NumericalFailure(f"non-finite wave speed at t = {self.t:.3f} s")
         if status == _lib.EDTMIN:

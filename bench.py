@@ -929,6 +929,8 @@ def main() -> None:
     kernel = f"{args.arith}::strips_kernel<{form}>" if form else f"{args.arith}::faces_kernel"
     roofline = {"kernel": kernel, "bound": "hbm", "achieved": achieved, "peak": hbm, "unit": "GB/s",
                 "frac": achieved / hbm, "peak_kind": peak_kind, "traffic": traffic,
+                # the DRAM bytes the launch moves (traffic, from the capture) over its time, against the same peak
+                "traffic_frac": traffic / (faces / 1e3) / 1e9 / hbm,
                 "alg_bytes_per_cell": ALG_FACES, "launch_ms": faces,
                 "update_kernel_ms": statistics.mean(update_ms),
                 "step_alg_bytes_per_cell": ALG_STEP,

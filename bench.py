@@ -14,8 +14,8 @@ all ranks (ranks run independent replicas: weak scaling, no collective in the da
 kernel (the face pass) from CUDA events; parity = the timed build against the oracle on a block of the workload;
 cpu_baseline = the oracle (a C restatement of the reference's CPU step) on that block; e2e = the same metric through
 the C-ABI with host buffers (per 30 s window, as the reference's run driver and monitor take a run: the window's rain
-uploaded from pinned memory, the window stepped, the clock, active list, design-line discharge, outfall volume and
-storage read back; the envelope maps at the end); sweep = the critical-duration search at a reduced size.
+uploaded from pinned memory a window ahead, the window stepped, the clock, active list, design-line discharge, outfall
+volume and storage read back; the envelope maps at the end); sweep = the critical-duration search at a reduced size.
 
 ``--impl reference`` times the reference's CPU step (its restatement, the oracle, with every host thread) on the
 same bounded block and prints the same line with "impl": "reference".

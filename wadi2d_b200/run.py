@@ -153,6 +153,8 @@ class SourceStager:
         """Start the copy of ``rates`` (a pinned host tensor of the NATIVE field's size); returns its bytes."""
         if rates.numel() != self.buf.numel() or rates.dtype != self.torch.float32:
             raise ValueError(f"stage: {rates.numel()} {rates.dtype} values for {self.buf.numel()} float32")
+        if self.pending:
+            raise RuntimeError("stage: the rates staged before have not been committed")
         cur = self.torch.cuda.current_stream(self.b.device)
         self.side.wait_stream(cur)  # the buffer's last commit has been copied out
         with self.torch.cuda.stream(self.side):

@@ -71,7 +71,9 @@ def parse():
     p.add_argument("--n", type=int, default=4096, help="domain side in cells (configuration 3: 4096)")
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--e2e-windows", type=int, default=16)
+    p.add_argument("--e2e-windows", type=int, default=64,
+                   help="30 s windows of the end-to-end leg (a 36 h run has 4,320; the envelope maps are read once, "
+                        "at the end, as a run reads them)")
     p.add_argument("--full-run", action="store_true",
                    help="the whole 36 h run of configuration 3 from dry ground, with its mass balance")
     p.add_argument("--sim-hours", type=float, default=36.0, help="--full-run: simulated hours (configuration 3: 36)")

@@ -429,6 +429,10 @@ int32_t w2b_colsum_bf16(const void* x, int32_t rows, int32_t cols, float* out, v
  * (BF16, or NULL) = the new weights. */
 int32_t w2b_adam(float* w, const float* g, float* m, float* v, int64_t n, float lr_t, float b1, float b2, float eps,
                  void* wb, void* stream);
+/* w2b_adam with the step size read on the device: lr_t = lr_table[*step] (step: a device int64). A training step
+ * captured once in a CUDA graph then replays with each step's own bias-corrected size. */
+int32_t w2b_adam_table(float* w, const float* g, float* m, float* v, int64_t n, const float* lr_table,
+                       const int64_t* step, float b1, float b2, float eps, void* wb, void* stream);
 
 #ifdef __cplusplus
 }

@@ -47,3 +47,25 @@ def test_training_fits_a_smooth_map():
     assert losses[-1] < 0.05 * losses[0]
     err = np.mean((net.predict(x[896:]) - t[896:]) ** 2)
     assert err < 0.25  # held-out rows: the mean alone scores 1 on standardised targets
+
+
+def test_training_replayed_as_a_graph_equals_stepping_from_the_host():
+    """The captured training step, replayed with each step's batch and step size read on the device, gives the same
+    weights, bit for bit, and the same losses as the same steps launched one by one from the host."""
+    from wadi2d_b200.surrogate import Network
+
+    rng = np.random.default_rng(8)
+    x = rng.standard_normal((300, 16)).astype(np.float32)
+    t = rng.standard_normal((300, 16)).astype(np.float32)
+    nets = [Network(seed=4), Network(seed=4)]
+    lg = nets[0].fit(x, t, iters=250, batch=96, seed=6, graph=True)
+    lh = nets[1].fit(x, t, iters=250, batch=96, seed=6, graph=False)
+    assert lg == lh
+    for (wg, bg), (wh, bh) in zip(nets[0].weights(), nets[1].weights(), strict=True):
+        assert np.array_equal(wg, wh) and np.array_equal(bg, bh)
+    assert nets[0].t == nets[1].t == 250
+    # a second fit continues the step count and the moments the same way
+    lg = nets[0].fit(x, t, iters=120, batch=96, seed=7, graph=True)
+    lh = nets[1].fit(x, t, iters=120, batch=96, seed=7, graph=False)
+    assert lg == lh
+    assert all(np.array_equal(a[0], b[0]) for a, b in zip(nets[0].weights(), nets[1].weights(), strict=True))

@@ -121,6 +121,7 @@ _SIGNATURES = {
     "w2b_mse_grad": [c_vp, c_vp, c_i32, c_i32, c_i32, c_f32, c_vp, c_vp, c_vp],
     "w2b_colsum_bf16": [c_vp, c_i32, c_i32, c_vp, c_vp],
     "w2b_adam": [c_vp, c_vp, c_vp, c_vp, c_i64, c_f32, c_f32, c_f32, c_f32, c_vp, c_vp],
+    "w2b_adam_table": [c_vp, c_vp, c_vp, c_vp, c_i64, c_vp, c_vp, c_f32, c_f32, c_f32, c_vp, c_vp],
     "w2b_source_runs": [c_vp, c_i64, c_vp, c_vp, c_vp],
     "w2b_set_lines": [c_vp, c_i32, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp, c_vp],
     "w2b_advance_runs": [c_vp, ctypes.POINTER(Stepper), c_vp, c_i64, c_vp, c_vp],

@@ -199,10 +199,14 @@ __global__ void colsum_kernel(const __nv_bfloat16* __restrict__ x, int rows, int
     out[c] = s;
 }
 
-// Adam on FP32 weights (bias-corrected steps lr_t = lr sqrt(1 - b2^t) / (1 - b1^t)), and their BF16 copy
+// Adam on FP32 weights (bias-corrected steps lr_t = lr sqrt(1 - b2^t) / (1 - b1^t)), and their BF16 copy. With
+// lr_table, the step size is lr_table[*step], read on the device (a captured training step replays with each step's
+// own size).
 __global__ void adam_kernel(float* __restrict__ w, const float* __restrict__ g, float* __restrict__ m,
-                            float* __restrict__ v, int64_t n, float lr_t, float b1, float b2, float eps,
+                            float* __restrict__ v, int64_t n, float lr_t, const float* __restrict__ lr_table,
+                            const int64_t* __restrict__ step, float b1, float b2, float eps,
                             __nv_bfloat16* __restrict__ wb) {
+    if (lr_table) lr_t = lr_table[*step];
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const float gi = g[i];
         const float mi = b1 * m[i] + (1.0f - b1) * gi;
@@ -276,7 +280,15 @@ int32_t w2b_colsum_bf16(const void* x, int32_t rows, int32_t cols, float* out, v
 int32_t w2b_adam(float* w, const float* g, float* m, float* v, int64_t n, float lr_t, float b1, float b2, float eps,
                  void* wb, void* stream) {
     if (!w || !g || !m || !v || n < 0) return W2B_EINVAL;
-    adam_kernel<<<296, 256, 0, (cudaStream_t)stream>>>(w, g, m, v, n, lr_t, b1, b2, eps,
+    adam_kernel<<<296, 256, 0, (cudaStream_t)stream>>>(w, g, m, v, n, lr_t, nullptr, nullptr, b1, b2, eps,
+                                                       static_cast<__nv_bfloat16*>(wb));
+    return cudaGetLastError() == cudaSuccess ? W2B_OK : W2B_ECUDA;
+}
+
+int32_t w2b_adam_table(float* w, const float* g, float* m, float* v, int64_t n, const float* lr_table,
+                       const int64_t* step, float b1, float b2, float eps, void* wb, void* stream) {
+    if (!w || !g || !m || !v || !lr_table || !step || n < 0) return W2B_EINVAL;
+    adam_kernel<<<296, 256, 0, (cudaStream_t)stream>>>(w, g, m, v, n, 0.0f, lr_table, step, b1, b2, eps,
                                                        static_cast<__nv_bfloat16*>(wb));
     return cudaGetLastError() == cudaSuccess ? W2B_OK : W2B_ECUDA;
 }

@@ -105,8 +105,10 @@ class Network:
         return out
 
     def _input(self, x):
+        """Standardised inputs (host array, or FP32 on the device) padded to 16 rows and cast to BF16."""
         torch = self.torch
-        x = torch.as_tensor(np.asarray(x, np.float32), device=self.device)
+        if not (isinstance(x, torch.Tensor) and x.is_cuda):
+            x = torch.as_tensor(np.asarray(x, np.float32), device=self.device)
         n = x.shape[0]
         npad = _pad16(max(n, 1))
         xp = torch.zeros((npad, self.dims[0]), dtype=torch.float32, device=self.device)
@@ -137,7 +139,9 @@ class Network:
         torch = self.torch
         y, (n, npad, hs, zs) = self.forward(x, keep=True)
         tt = torch.zeros((npad, self.dims[-1]), dtype=torch.float32, device=self.device)
-        tt[:n] = torch.as_tensor(np.asarray(t, np.float32), device=self.device)
+        if not (isinstance(t, torch.Tensor) and t.is_cuda):
+            t = torch.as_tensor(np.asarray(t, np.float32), device=self.device)
+        tt[:n] = t
         yp = zs[-1]
         nout = self.dims[-1]
         dz = torch.empty((npad, nout), dtype=torch.bfloat16, device=self.device)
@@ -159,32 +163,78 @@ class Network:
                 _lib.call("w2b_relu_back", g.data_ptr(), zs[i - 1].data_ptr(), g.numel(), dz.data_ptr(), self._s())
         return loss, gW, gb
 
-    def step(self, x, t, b1: float = 0.9, b2: float = 0.999, eps: float = 1e-8):
+    def _lr(self, t: int, b1: float = 0.9, b2: float = 0.999) -> float:
+        """Adam's bias-corrected step size at step t."""
+        return float(self.lr * np.sqrt(1.0 - b2**t) / (1.0 - b1**t))
+
+    def _adam(self, gW, gb, lr_t: float = 0.0, table=None, b1: float = 0.9, b2: float = 0.999, eps: float = 1e-8):
+        """Adam on every layer with step size lr_t, or (table) lr_table[*step] read on the device."""
+        for i in range(len(self.W)):
+            for w, g, m, v in ((self.W[i], gW[i], self.mW[i], self.vW[i]), (self.b[i], gb[i], self.mb[i], self.vb[i])):
+                if table is None:
+                    _lib.call("w2b_adam", w.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr(), w.numel(), lr_t, b1,
+                              b2, eps, None, self._s())  # fmt: skip
+                else:
+                    _lib.call("w2b_adam_table", w.data_ptr(), g.data_ptr(), m.data_ptr(), v.data_ptr(), w.numel(),
+                              table[0].data_ptr(), table[1].data_ptr(), b1, b2, eps, None, self._s())  # fmt: skip
+            self._sync(i)
+
+    def _check(self) -> None:
+        if int(self.status.item()) != 0:
+            raise _lib.W2BError(int(self.status.item()), "w2b_mma_gemm")
+
+    def step(self, x, t):
         """One Adam step on the batch (x, t); returns the loss before the step (a device scalar)."""
         loss, gW, gb = self.gradients(x, t)
         self.t += 1
-        lr_t = self.lr * np.sqrt(1.0 - b2**self.t) / (1.0 - b1**self.t)
-        for i in range(len(self.W)):
-            _lib.call("w2b_adam", self.W[i].data_ptr(), gW[i].data_ptr(), self.mW[i].data_ptr(), self.vW[i].data_ptr(),
-                      self.W[i].numel(), float(lr_t), b1, b2, eps, None, self._s())  # fmt: skip
-            _lib.call("w2b_adam", self.b[i].data_ptr(), gb[i].data_ptr(), self.mb[i].data_ptr(), self.vb[i].data_ptr(),
-                      self.b[i].numel(), float(lr_t), b1, b2, eps, None, self._s())  # fmt: skip
-            self._sync(i)
-        if int(self.status.item()) != 0:
-            raise _lib.W2BError(int(self.status.item()), "w2b_mma_gemm")
+        self._adam(gW, gb, self._lr(self.t))
+        self._check()
         return loss
 
-    def fit(self, x, t, iters: int = 2000, batch: int = 256, seed: int = 0) -> list[float]:
-        """Adam over random batches of (x, t), standardised; returns the loss every 100 steps."""
+    def fit(self, x, t, iters: int = 2000, batch: int = 256, seed: int = 0, graph: bool = True) -> list[float]:
+        """Adam over random batches of (x, t), standardised; returns the loss every 100 steps.
+
+        With ``graph`` (the default) the batches are drawn up front (the same draws, in the same order, as one step
+        at a time draws them), the training set goes to the device once, and one step (gather, forward, backward,
+        Adam with the step's own size read on the device) is captured as a CUDA graph after a first step run eagerly,
+        then replayed: the same kernels on the same data in the same order as stepping from the host, without a host
+        round trip a step."""
         rng = np.random.default_rng(seed)
         x, t = np.asarray(x, np.float32), np.asarray(t, np.float32)
-        losses = []
-        for it in range(iters):
-            idx = rng.choice(x.shape[0], size=min(batch, x.shape[0]), replace=False)
-            loss = self.step(x[idx], t[idx])
-            if it % 100 == 0 or it == iters - 1:
-                losses.append(float(loss))
-        return losses
+        bs = min(batch, x.shape[0])
+        draws = [rng.choice(x.shape[0], size=bs, replace=False) for _ in range(iters)]
+        if not graph or iters < 2:
+            losses = []
+            for it in range(iters):
+                loss = self.step(x[draws[it]], t[draws[it]])
+                if it % 100 == 0 or it == iters - 1:
+                    losses.append(float(loss))
+            return losses
+        torch, dev = self.torch, self.device
+        X, T = torch.as_tensor(x, device=dev), torch.as_tensor(t, device=dev)
+        idx = torch.as_tensor(np.stack(draws).astype(np.int64), device=dev)
+        lr = torch.as_tensor(np.array([self._lr(self.t + s) for s in range(1, iters + 1)], np.float32), device=dev)
+        k = torch.zeros(1, dtype=torch.int64, device=dev)
+        loss_at = torch.zeros(iters, dtype=torch.float64, device=dev)
+
+        def one() -> None:
+            rows = idx.index_select(0, k).view(-1)
+            loss, gW, gb = self.gradients(X.index_select(0, rows), T.index_select(0, rows))
+            self._adam(gW, gb, table=(lr, k))
+            loss_at.index_copy_(0, k, loss.view(1).to(torch.float64))
+            k.add_(1)
+
+        one()  # the first step, from the host: every kernel's first launch happens outside the capture
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g):
+            one()
+        for _ in range(iters - 1):
+            g.replay()
+        self.t += iters
+        self._check()
+        del g
+        out = loss_at.cpu().numpy()
+        return [float(out[it]) for it in range(iters) if it % 100 == 0 or it == iters - 1]
 
     def predict(self, x) -> np.ndarray:
         return self.forward(x).cpu().numpy().astype(np.float64)

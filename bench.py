@@ -944,7 +944,7 @@ def main() -> None:
     # clock and the active list, the design line's discharge, the outfall volume, the FP64 storage); at the end the
     # five envelope maps
     from wadi2d_b200.maxima import Lines, faces_across
-    from wadi2d_b200.run import DeviceStorage, SourceStager
+    from wadi2d_b200.run import DeviceStorage, MonitorReads, SourceStager
     from wadi2d_b200.state import state_index
 
     rows, cols = c.boundary_cells()
@@ -960,7 +960,8 @@ def main() -> None:
     h2d = d2h = 0
     # the monitor's reads once before the timed region, as the steps are warmed: their kernels' first launches (about
     # 20 ms, once a process) belong to a run's set-up, not to each of its thousands of windows
-    line.discharge(), tally.volume(), storage()
+    monitor = MonitorReads(m, line, tally, storage)  # the three reads behind one synchronisation
+    monitor()
     torch.cuda.synchronize(dev)
     w0 = time.perf_counter()
     s0 = m.stepper.nsteps
@@ -973,8 +974,9 @@ def main() -> None:
             h2d += stager.stage(src_native)  # the next window's, crossing while this one steps
         m.run(m.stepper.t + win, maxima=maxima, tally=tally)
         d2h += ctypes.sizeof(_lib.Clock) + 4 * (int(b.nact) + grid.ntiles)  # the clock, the active list, idle counts
-        series.append((m.stepper.t, float(line.discharge()[0]), tally.volume(), storage()))
-        d2h += 8 * 3
+        q, outflow, stored = monitor()
+        series.append((m.stepper.t, float(q[0]), outflow, stored))
+        d2h += monitor.host.numel() * 8
     for dst, a in zip(env_host, maxima.arrays, strict=True):
         dst.copy_(a, non_blocking=True)
     d2h += sum(a.numel() * a.element_size() for a in env_host)

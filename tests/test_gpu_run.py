@@ -231,3 +231,32 @@ def test_staged_source_windows_equal_the_synchronous_upload():
     assert a.stepper.nsteps == b.stepper.nsteps > 6
     for name in ("h", "d", "u", "v", "qx", "qy", "mx", "my", "src"):
         assert np.array_equal(a.field(name), b.field(name)), name
+
+
+def test_monitor_reads_in_one_round_trip_equal_the_reads_one_by_one():
+    """MonitorReads (the design lines' discharge, the outfall volume and the FP64 storage behind one
+    synchronisation) gives exactly what Lines.discharge, Tally.volume and DeviceStorage give, window after window."""
+    from wadi2d_b200.maxima import Lines, faces_across
+    from wadi2d_b200.run import MonitorReads
+
+    w, og, g, tab = c1(64)
+    m = Model(GridTables.from_dict(g, tab), Numerics(arithmetic="fast"))
+    m.set_depth(np.where(g.mask, 0.02, 0.0))
+    rate = np.zeros(g.shape)
+    rate[1 : 1 + w.ny, 1 : w.nx] = w.rain_mm_h / 3.6e6
+    m.set_source(rate)
+    rows, cols = w.outfall
+    outfall = np.array([m.cell_state_index(int(j), int(i)) for j, i in zip(rows, cols, strict=True)], np.int64)
+    tally = Tally(m, outfall, np.ones(outfall.size), np.zeros(0, np.int64), np.zeros(0))
+    line = Lines(m, [faces_across(g, np.full(20, 30), np.arange(20, 40), axis=0),
+                     faces_across(g, np.full(10, 50), np.arange(5, 15), axis=0)])  # fmt: skip
+    jj, ii = np.nonzero(g.mask)
+    storage = DeviceStorage(m, state_index(g, jj, ii).astype(np.int64))
+    monitor = MonitorReads(m, line, tally, storage)
+    for k in range(1, 5):
+        m.run(60.0 * k, tally=tally)
+        q, outflow, stored = monitor()
+        assert np.array_equal(q, line.discharge())
+        assert outflow == tally.volume()
+        assert stored == storage()
+    assert stored > 0.0

@@ -122,6 +122,10 @@ class Lines:
         """Each line's discharge after the last step, m3/s."""
         return self._t[4][: self.n].cpu().numpy()
 
+    def discharge_device(self):
+        """The same, as the device FP64 tensor (no copy to the host)."""
+        return self._t[4][: self.n]
+
     def peaks(self) -> tuple[np.ndarray, np.ndarray]:
         """Each line's peak |Q| (m3/s) and the time it was reached (s)."""
         return self._t[5][: self.n].cpu().numpy(), self._t[6][: self.n].cpu().numpy()

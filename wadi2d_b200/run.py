@@ -126,11 +126,46 @@ class DeviceStorage:
         self.partial = torch.zeros(_lib.PARTIALS, dtype=torch.float64, device=b.device)
         self.out = torch.zeros(1, dtype=torch.float64, device=b.device)
 
-    def __call__(self) -> float:
+    def launch(self) -> None:
+        """The storage into ``out`` (a device FP64 scalar), on the current stream, without waiting for it."""
         b = self.model.backend
         _lib.call("w2b_storage", b.handle, int(self.cells.numel()), self.cells.data_ptr(), self.partial.data_ptr(),
                   self.out.data_ptr(), b._stream())  # fmt: skip
+
+    def __call__(self) -> float:
+        self.launch()
         return float(self.out.item())
+
+
+class MonitorReads:
+    """What the run driver's monitor reads after each window (wadi2d/engine/monitor.py:197-218, :229-232), in one
+    round trip: each design line's discharge, the outfall volume and the FP64 storage are queued on the current stream
+    into one pinned buffer and read after a single synchronisation, where reading them one by one waits on the device
+    once each. The figures are the same as ``Lines.discharge``, ``Tally.volume`` and ``DeviceStorage`` give."""
+
+    def __init__(self, model, lines=None, tally=None, storage=None) -> None:
+        b = model.backend
+        self.b, self.torch = b, b.torch
+        self.lines, self.tally, self.storage = lines, tally, storage
+        self.nl = 0 if lines is None else int(lines.n)
+        self.buf = self.torch.zeros(self.nl + 2, dtype=self.torch.float64, device=b.device)
+        self.host = self.torch.zeros(self.nl + 2, dtype=self.torch.float64).pin_memory()
+
+    def __call__(self) -> tuple[np.ndarray, float, float]:
+        """(each line's discharge m3/s, the outfall volume m3, the storage m3); 0 for what was not given."""
+        nl, buf = self.nl, self.buf
+        if nl:
+            buf[:nl].copy_(self.lines.discharge_device())
+        if self.tally is not None and self.tally.n:
+            buf[nl].copy_(self.tally.total.sum())
+        if self.storage is not None:
+            self.storage.launch()
+            buf[nl + 1].copy_(self.storage.out[0])
+        self.host.copy_(buf, non_blocking=True)
+        self.torch.cuda.current_stream(self.b.device).synchronize()
+        h = self.host.numpy()
+        outflow = 0.0 if self.tally is None else (self.tally.held + float(h[nl]) if self.tally.n else self.tally.held)
+        return h[:nl].copy(), outflow, float(h[nl + 1])
 
 
 class SourceStager:

@@ -120,6 +120,14 @@ typedef struct {
      * one copy: the arrays then hold only the distinct tiles (tile 0 the void tile), and table_tile maps each tile of
      * the batch to its catchment tile. No counterpart in the reference, which copies the tables into every run. */
     const int32_t *table_tile;
+    /* The update pass's level cache, (ntiles, 32, 32) cells each, in tile order (not table_tile's): every cell's last
+     * pair of level-table values (lpair, 2 floats a cell, 16-byte aligned) and its row (lrow, one byte a cell, 0xff:
+     * none). w2b_create sets every row to 0xff. A cell whose new row is the cached one takes the cached pair, copied
+     * into shared memory with the tile (coalesced), and the others gather from the table and cache what they read,
+     * so the results are the table's, bit for bit. From one step to the next about one cell in 700 changes row. Valid
+     * for the packed tables the handle was created with. No counterpart in the reference, which gathers every step. */
+    float *lpair;
+    uint8_t *lrow;
 } W2BBuffers;
 
 #define W2B_CTL_BYTES 1024

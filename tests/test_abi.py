@@ -74,7 +74,7 @@ def test_every_entry_point_refuses_null_arguments_without_a_gpu():
         zeros = [0.0 if a in (ctypes.c_float, ctypes.c_double) else (0 if a in (ctypes.c_int32, ctypes.c_int64,
                  ctypes.c_uint32) else None) for a in args]  # fmt: skip
         assert getattr(L, name)(*zeros) == _lib.EINVAL, name
-    assert L.w2b_version() == 2
+    assert L.w2b_version() == 3
     assert L.w2b_run_table_bytes(0) == 0
 
 

@@ -52,6 +52,7 @@ class Buffers(ctypes.Structure):
         + [(n, c_vp) for n in ("tiles", "tile_of", "nbr", "active", "wave", "wet", "keep", "idle", "is_act", "woken",
                                "work", "scratch", "bmark")]  # fmt: skip
         + [("env", c_vp * 5), ("ctl", c_vp), ("runs", c_vp), ("tile_run", c_vp), ("stage", c_vp), ("table_tile", c_vp)]
+        + [("lpair", c_vp), ("lrow", c_vp)]
     )
 
 

@@ -207,6 +207,8 @@ class B200Backend:
         t["tile_run"] = (torch.zeros(nt, dtype=torch.int32, device=dev) if tile_run is None
                          else torch.as_tensor(np.ascontiguousarray(tile_run, np.int32), device=dev))  # fmt: skip
         t["stage"] = f32(nt * STRIDE2)
+        t["lpair"] = f32(nt * TILE2 * 2)  # the update pass's level cache (w2b_create marks it empty)
+        t["lrow"] = torch.full((nt * TILE2,), 255, dtype=torch.uint8, device=dev)
         if table_tile is not None:
             tt = np.ascontiguousarray(table_tile, np.int32)
             if tt.shape != (nt,) or tt.min() < 0 or tt.max() >= ntab or tt[0] != 0:
@@ -239,7 +241,7 @@ class B200Backend:
             getattr(B, n)[1] = t[n][1].data_ptr()
         for n in ("d", "qx", "qy", "qx1", "qy1", "res", "src", "om", "zcx", "zcy", "hc", "dtab2", "tiles", "tile_of",
                   "nbr", "active", "wave", "wet", "keep", "idle", "is_act", "woken", "work", "scratch", "bmark", "ctl",
-                  "runs", "tile_run", "stage"):  # fmt: skip
+                  "runs", "tile_run", "stage", "lpair", "lrow"):  # fmt: skip
             setattr(B, n, t[n].data_ptr())
         for a, ax in enumerate("xy"):
             for f in ("fl", "fr", "gl", "gr", "ef", "cw"):

@@ -215,6 +215,8 @@ static StepArgs make_args(const Handle& H) {
     A.ltime = H.ltime;
     A.ctl = H.ctl();
     A.tile_run = H.B.tile_run;
+    A.lpair = reinterpret_cast<float2*>(H.B.lpair);
+    A.lrow = H.B.lrow;
     A.R = H.R;
     A.nruns = H.nruns;
     return A;
@@ -432,7 +434,7 @@ using namespace w2b;
 
 extern "C" {
 
-int32_t w2b_version(void) { return 2; }
+int32_t w2b_version(void) { return 3; }
 
 int64_t w2b_run_table_bytes(int32_t nruns) { return nruns < 1 ? 0 : (int64_t)run_table_bytes(nruns); }
 
@@ -485,7 +487,7 @@ int32_t w2b_create(const W2BGridDesc* grid, const W2BParams* params, const W2BBu
     {
         // arrays the passes stage with bulk copies: 16-byte aligned
         auto a16 = [](const void* q) { return q && !((uintptr_t)q & 15); };
-        bool ok = a16(buffers->hc);
+        bool ok = a16(buffers->hc) && a16(buffers->lpair) && a16(buffers->lrow);
         for (int x = 0; x < 2; ++x)
             ok = ok && a16(buffers->fl[x]) && a16(buffers->fr[x]) && a16(buffers->gl[x]) && a16(buffers->gr[x]) &&
                  a16(buffers->ef[x]) && a16(buffers->cw[x]);
@@ -515,6 +517,11 @@ int32_t w2b_create(const W2BGridDesc* grid, const W2BParams* params, const W2BBu
     H->nact = grid->ntiles - 1;
     H->nruns = grid->nruns;
     H->R = run_table(H->B.runs, H->nruns);
+    // the level cache holds nothing yet: every row 0xff
+    if (cudaMemset(H->B.lrow, 0xff, (size_t)H->g.ntiles * TILE2) != cudaSuccess) {
+        delete H;
+        return cuda_status(cudaGetLastError(), "w2b_create level cache");
+    }
     const int32_t stored = 1;  // the caller's momentum arrays hold the momenta the first step starts from
     if (cudaMemcpy(&H->ctl()->m_stored, &stored, sizeof(stored), cudaMemcpyHostToDevice) != cudaSuccess) {
         delete H;

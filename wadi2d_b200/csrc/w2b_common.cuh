@@ -156,6 +156,9 @@ struct StepArgs {
     // runs: the run of each tile, and the run table
     const int32_t* __restrict__ tile_run;
     RunTab R;
+    // the update pass's level cache: each cell's last level pair and its row (0xff: none), tile layout
+    float2* __restrict__ lpair;
+    uint8_t* __restrict__ lrow;
     int32_t nruns;
 };
 

@@ -742,8 +742,11 @@ constexpr int RPAD = RING + 1;
 constexpr int U_QX1 = 0, U_QY1 = 1, U_H = 2;       // 40 x 36 boxes
 constexpr int U_OWN = 3 * BOX;                      // res, src, hc: 32 x 32 each
 constexpr int U_R = U_OWN + 3 * TILE2;              // r of the tile and its ring
-constexpr int U_FLOATS = U_R + RING * RPAD;
-constexpr int UPDATE_SMEM = U_FLOATS * 4;           // 34,328 bytes
+constexpr int U_LP = (U_R + RING * RPAD + 31) / 32 * 32;  // the tile's cached level pairs (float2), 128-byte aligned
+constexpr int U_LR = U_LP + 2 * TILE2;                     // and their rows (bytes)
+constexpr int U_FLOATS = U_LR + TILE2 / 4;
+constexpr int UPDATE_SMEM = U_FLOATS * 4;           // 43,648 bytes: four CTAs a SM
+static_assert(UPDATE_SMEM == 43648, "update image size");
 constexpr int UPDATE_THREADS = 256;
 
 // The first entry at or after a, in steps of the grid, whose run is stepping (the same for every thread of a CTA).
@@ -754,12 +757,12 @@ __device__ __forceinline__ int next_tile(const StepArgs& A, int a, int nwork) {
 }
 
 // Issue (thread 0) the copies of tile t's update image against bar: the unscaled discharges and the old depth with
-// their ring, the residual, the source and Hc.
+// their ring, the residual, the source and Hc, and the tile's level cache (each cell's last level pair and its row).
 __device__ __forceinline__ void update_issue(float* sm, uint64_t* bar, const TMaps& M, const StepArgs& A, int t) {
     const int p = A.R.parity[A.tile_run[t]];
     const int tj = A.tiles[2 * t], ti = A.tiles[2 * t + 1];
     fence_proxy_async();
-    mbar_expect_tx(bar, (uint32_t)(3 * BOX + 3 * TILE2) * 4u);
+    mbar_expect_tx(bar, (uint32_t)(3 * BOX + 3 * TILE2) * 4u + (uint32_t)TILE2 * 9u);
     const int x0 = ti * TILE + GX - 4, y0 = tj * TILE + GY - 2;
     tma_load_2d(sm + U_QX1 * BOX, &M.qx1, x0, y0, bar);
     tma_load_2d(sm + U_QY1 * BOX, &M.qy1, x0, y0, bar);
@@ -767,13 +770,16 @@ __device__ __forceinline__ void update_issue(float* sm, uint64_t* bar, const TMa
     tma_load_2d(sm + U_OWN, &M.res, x0 + 4, y0 + 2, bar);
     tma_load_2d(sm + U_OWN + TILE2, &M.src, x0 + 4, y0 + 2, bar);
     bulk_load(sm + U_OWN + 2 * TILE2, A.hc + (size_t)table_of(A, t) * TILE2, TILE2 * 4, bar);
+    bulk_load(sm + U_LP, A.lpair + (size_t)t * TILE2, TILE2 * 8, bar);
+    bulk_load(sm + U_LR, A.lrow + (size_t)t * TILE2, TILE2, bar);
 }
 
 // The update pass (wadi2d/solver/gpu/kernels/cells.cu:4-63 with limit fused in): TMA stages the tile's unscaled
-// discharges and old depth with their ring, its residual, source and Hc; r of the tile and its one-cell ring is
-// formed in shared memory; then each thread takes its four cells through continuity and issues their four
-// level-table loads together. Once every thread has read the image, thread 0 issues the next tile's copies into it,
-// and they land while the gathers return and the level, the wet share and the wet flag are finished.
+// discharges and old depth with their ring, its residual, source and Hc, and its level cache; r of the tile and its
+// one-cell ring is formed in shared memory; then each thread takes its four cells through continuity and takes their
+// level pairs from the cache, or for the cells whose row changed from the table (the gathers issued together). Once
+// every thread has read the image, thread 0 issues the next tile's copies into it, and they land while any gathers
+// return and the level, the wet share and the wet flag are finished.
 __global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_constant__ TMaps M, StepArgs A) {
     extern __shared__ __align__(128) float sm[];
     __shared__ __align__(8) uint64_t bar;
@@ -868,11 +874,23 @@ __global__ void __launch_bounds__(UPDATE_THREADS) update_kernel(const __grid_con
                 rr[c] = row_of(sv[c], last);
             }
         }
+        // the level pairs: the cached one where the cell's row is the cached row (about 699 cells in 700 from one
+        // step to the next), else gathered from the table and cached
         float2 pr[4];
+        const float2* LP = reinterpret_cast<const float2*>(sm + U_LP);
+        const uint8_t* LR = reinterpret_cast<const uint8_t*>(sm + U_LR);
 #pragma unroll
         for (int c = 0; c < 4; ++c) {
             const int local = (threadIdx.y * 4 + c) * TILE + threadIdx.x;
-            pr[c] = rr[c] >= 0 ? __ldg(pairs_t + (size_t)rr[c] * TILE2 + local) : make_float2(0.0f, 0.0f);
+            if (rr[c] < 0) {
+                pr[c] = make_float2(0.0f, 0.0f);
+            } else if (LR[local] == rr[c]) {
+                pr[c] = LP[local];
+            } else {
+                pr[c] = __ldg(pairs_t + (size_t)rr[c] * TILE2 + local);
+                A.lpair[(size_t)t * TILE2 + local] = pr[c];
+                A.lrow[(size_t)t * TILE2 + local] = (uint8_t)rr[c];
+            }
         }
         // every thread has read the image and r: the next tile's copies land in it during this tile's gathers
         __syncthreads();

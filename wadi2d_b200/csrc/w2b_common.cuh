@@ -273,19 +273,25 @@ __device__ __forceinline__ float cbrt_fast(float x) {
     const float y = fmaf(-fmaf(p, y0, -x), rcp_approx(3.0f * p), y0);
     return y0 > 0.0f ? y : y0;
 }
+// Python max/min on two ordered floats (the first argument wins a tie).
+__device__ __forceinline__ float fmax32(float a, float b) { return a >= b ? a : b; }
+__device__ __forceinline__ float fmin32(float a, float b) { return a <= b ? a : b; }
+
 #ifdef W2B_FAST
 __device__ __forceinline__ float qdiv(float a, float b) { return __fdividef(a, b); }
 __device__ __forceinline__ float qsqrt(float x) { return sqrt_approx(x); }
 __device__ __forceinline__ float qcbrt(float x) { return cbrt_fast(x); }
+// the hardware max and min, one instruction each: the same as fmax32 / fmin32 for ordered operands but for the sign of
+// a zero tie, and they return the other operand where one is NaN
+__device__ __forceinline__ float qmax(float a, float b) { return fmaxf(a, b); }
+__device__ __forceinline__ float qmin(float a, float b) { return fminf(a, b); }
 #else
 __device__ __forceinline__ float qdiv(float a, float b) { return a / b; }
 __device__ __forceinline__ float qsqrt(float x) { return sqrtf(x); }
 __device__ __forceinline__ float qcbrt(float x) { return cbrt32(x); }
+__device__ __forceinline__ float qmax(float a, float b) { return fmax32(a, b); }
+__device__ __forceinline__ float qmin(float a, float b) { return fmin32(a, b); }
 #endif
-
-// Python max/min on two ordered floats (the first argument wins a tie).
-__device__ __forceinline__ float fmax32(float a, float b) { return a >= b ? a : b; }
-__device__ __forceinline__ float fmin32(float a, float b) { return a <= b ? a : b; }
 
 __device__ __forceinline__ float minmod(float a, float b) {
     if (a * b <= 0.0f) return 0.0f;

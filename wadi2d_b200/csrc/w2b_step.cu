@@ -19,7 +19,8 @@ namespace w2b {
 
 // The face and update passes are compiled twice (wadi2d_b200/build.py): into namespace exact with the library's IEEE
 // flags, the reference's float32 bits, and into namespace fast with W2B_FAST and FMA contraction (the approximate
-// division, square root and cube root of w2b_common.cuh qdiv/qsqrt/qcbrt). W2BParams.arith picks one per handle.
+// division, square root and cube root and the hardware max and min of w2b_common.cuh qdiv/qsqrt/qcbrt/qmax/qmin, in
+// the face arithmetic). W2BParams.arith picks one per handle.
 // Everything after them (envelope, boundary, control, converters) is compiled once, with the exact build.
 #ifdef W2B_FAST
 #define W2B_ARITH fast
@@ -121,8 +122,8 @@ __device__ __forceinline__ FaceIn face_in(const float* sm, int b, int sl) {
     I.e_l = D[b - S] - st[0 * L::S + sl];
     I.e_r = D[b] - st[1 * L::S + sl];
     I.uf = U[b];
-    I.e_lp = fmax32(I.e_l, 0.0f);
-    I.e_rp = fmax32(I.e_r, 0.0f);
+    I.e_lp = qmax(I.e_l, 0.0f);
+    I.e_rp = qmax(I.e_r, 0.0f);
     return I;
 }
 
@@ -207,9 +208,9 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int sl, int loc
             const float g_u = from_left ? st[2 * L::S + sl] : st[3 * L::S + sl];
             const float g_d = from_left ? st[3 * L::S + sl] : st[2 * L::S + sl];
             const float h_d = from_left ? h_r : h_l;
-            const float drop = (hup - g_u) - fmax32(h_d - g_d, HALF * (g_u - g_d));
+            const float drop = (hup - g_u) - qmax(h_d - g_d, HALF * (g_u - g_d));
             const float level_drop = fabsf(I.e_l - I.e_r);
-            const float drive = fmax32(eup, fmin32(drop, level_drop));
+            const float drive = qmax(eup, qmin(drop, level_drop));
             d_eta = from_left ? -drive : drive;
         }
     }
@@ -273,7 +274,7 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int sl, int loc
         const float a1 = q.z, a0 = q.x;
         w = qdiv(a1 - a0, top * rowc[2 * (A.rows - 1)]);
         area = a1 + w * (e - top);
-        tt = q.w * qdiv(area, fmax32(a1, 1e-12f));
+        tt = q.w * qdiv(area, qmax(a1, 1e-12f));
     } else {
         const int r = F.bits & FA_ROW;
         const float e0 = rowc[2 * r] * top;
@@ -296,7 +297,7 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int sl, int loc
     if (ON || P.sheet) {
         const float avol = hup * dx;
         if (avol < area) {
-            const float sub = qdiv(fmin32(I.e_lp, I.e_rp), fmax32(I.e_lp, I.e_rp));
+            const float sub = qdiv(qmin(I.e_lp, I.e_rp), qmax(I.e_lp, I.e_rp));
             const float sub2 = sub * sub;
             const float alpha = sub2 * sub2;
             rho = alpha + qdiv((ONE - alpha) * avol, area);
@@ -305,12 +306,12 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int sl, int loc
     // [5] friction. The fast build forms 1 / max(tt^(10/3), 1e-30) and 1 / max(rho^(4/3), 1e-12) as capped powers from
     // the hardware log2 and exp2 (within about 1e-6 relative; tt = 0 or rho = 0 gives the cap, as the clamps do).
 #ifdef W2B_FAST
-    float fric = area * area * fmin32(ex2_approx(-3.33333325f * lg2_approx(tt)), 1e30f);
-    if (rho < ONE) fric = fric * fmin32(ex2_approx(-1.33333337f * lg2_approx(rho)), 1e12f);
+    float fric = area * area * qmin(ex2_approx(-3.33333325f * lg2_approx(tt)), 1e30f);
+    if (rho < ONE) fric = fric * qmin(ex2_approx(-1.33333337f * lg2_approx(rho)), 1e12f);
 #else
     const float t3 = tt * tt * tt * qcbrt(tt);
-    float fric = qdiv(area * area, fmax32(t3, 1e-30f));
-    if (rho < ONE) fric = qdiv(fric, fmax32(rho * qcbrt(rho), 1e-12f));
+    float fric = qdiv(area * area, qmax(t3, 1e-30f));
+    if (rho < ONE) fric = qdiv(fric, qmax(rho * qcbrt(rho), 1e-12f));
 #endif
     const float a = dt * P.g * fric;
     const float sp = qsqrt(us * us + vb * vb);
@@ -328,10 +329,10 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int sl, int loc
             const float4* quads = A.ftab4[AX] + (size_t)t * (A.rows - 1) * TILE2 + local;
             face_lookup(eup + qdiv(HALF * ua * ua, P.g), top, quads, A.rows, area_c, tc, w_c);
         }
-        const float qc = c * area_c * qsqrt(qdiv(area_c, fmax32(w_c, 1e-9f)));
+        const float qc = c * area_c * qsqrt(qdiv(area_c, qmax(w_c, 1e-9f)));
         if (fabsf(qn) > qc) {
             qn = qn > ZERO ? qc : -qc;
-            un = qdiv(qn, fmax32(area * rho, 1e-12f));
+            un = qdiv(qn, qmax(area * rho, 1e-12f));
         }
     }
     if constexpr (PROBE) {
@@ -358,9 +359,9 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int sl, int loc
     }
     float plan = from_left ? om_l : om_r;
     const float dother = from_left ? d_right : d_left;
-    if (dother > P.h_cfl) plan = fmin32(plan, from_left ? om_r : om_l);
-    const float wave = qsqrt(fmax32(qdiv(P.g * area * rho, fmax32(plan, P.a_min) * dx), ZERO));
-    return fabsf(un) + fmin32(P.lead * fabsf(un - uf), 2.0f * wave) + wave;
+    if (dother > P.h_cfl) plan = qmin(plan, from_left ? om_r : om_l);
+    const float wave = qsqrt(qmax(qdiv(P.g * area * rho, qmax(plan, P.a_min) * dx), ZERO));
+    return fabsf(un) + qmin(P.lead * fabsf(un - uf), 2.0f * wave) + wave;
 }
 
 __device__ __forceinline__ float warp_max(float v) {

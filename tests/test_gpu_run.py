@@ -260,3 +260,25 @@ def test_monitor_reads_in_one_round_trip_equal_the_reads_one_by_one():
         assert outflow == tally.volume()
         assert stored == storage()
     assert stored > 0.0
+
+
+def test_level_cache_holds_the_tables_pairs():
+    """After a run, every cell that has a cached row holds the packed table's level pair at that row, bit for bit (the
+    update pass gathers from the table only where a cell's row changed and caches what it read)."""
+    w, og, g, tab = c1(64)
+    m = Model(GridTables.from_dict(g, tab), Numerics(arithmetic="fast"))
+    m.set_depth(np.where(g.mask, 0.05, 0.0))
+    rate = np.zeros(g.shape)
+    rate[1 : 1 + w.ny, 1 : w.nx] = w.rain_mm_h / 3.6e6
+    m.set_source(rate)
+    m.run(300.0)
+    b = m.backend
+    b.synchronize()
+    nt, rows = g.ntiles, int(m.tables.dtab.shape[-1])
+    row = b._t["lrow"].cpu().numpy().reshape(nt, 1024).astype(np.int64)
+    pair = b._t["lpair"].cpu().numpy().reshape(nt, 1024, 2)
+    table = b._t["dtab2"].cpu().numpy().reshape(nt, rows - 1, 1024, 2)
+    t, c = np.nonzero(row != 255)
+    assert t.size > 0.5 * (nt - 1) * 1024  # most wet cells have looked a row up
+    assert np.all(row[t, c] < rows - 1)
+    assert np.array_equal(pair[t, c].view(np.uint32), table[t, row[t, c], c].view(np.uint32))

@@ -10,6 +10,7 @@ Adam in FP32. Inputs and targets are standardised by the caller's statistics (``
 
 from __future__ import annotations
 
+import gc
 from dataclasses import dataclass
 
 import numpy as np
@@ -225,9 +226,19 @@ class Network:
             k.add_(1)
 
         one()  # the first step, from the host: every kernel's first launch happens outside the capture
+        # A finalizer that frees device memory (a solver backend dropped inside a reference cycle) must not run in the
+        # capture, which that call would end: collect first and keep the collector off until the capture is over.
+        # Thread-local capture: CUDA calls of other threads do not end it either.
+        gc.collect()
+        collecting = gc.isenabled()
+        gc.disable()
         g = torch.cuda.CUDAGraph()
-        with torch.cuda.graph(g):
-            one()
+        try:
+            with torch.cuda.graph(g, capture_error_mode="thread_local"):
+                one()
+        finally:
+            if collecting:
+                gc.enable()
         for _ in range(iters - 1):
             g.replay()
         self.t += iters

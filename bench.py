@@ -54,7 +54,7 @@ FALLBACK_HBM_GBS = 6650.0
 # their tile cells), from an ncu capture of fast::strips_kernel<8> (the form the tuner keeps) on configuration 3's
 # catchment at 1024 x 1024 cells (1,115,136 tile cells a launch, beyond L2): profiles/strips8_kernel_fast_config3_1024.md.
 # The traffic grows with the tile cells a launch processes, so it scales to this launch by them.
-FACES_DRAM_BYTES_PER_CELL = 166.6
+FACES_DRAM_BYTES_PER_CELL = 165.5
 CPU_BLOCK_TILES = 32  # the CPU sample: a 32 x 32-tile block (1,044,484 active cells) from the middle of the grid
 
 

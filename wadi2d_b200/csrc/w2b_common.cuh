@@ -255,16 +255,24 @@ __device__ __forceinline__ float cbrt32(float x) {
 // rounded cube root, so these are a / b, sqrtf and cbrt32. The step's second build (W2B_FAST, compiled with FMA
 // contraction; selected per handle by W2BParams.arith) uses the hardware's approximations where the face pass spends
 // its instructions:
-//  - division as __fdividef (rcp.approx times the numerator, within 2 ulp while the denominator's magnitude lies in
-//    [2^-126, 2^126]: every denominator of the face pass is a depth, area, width, cell size or clamp of them, bounded
-//    below by 1e-30 or by e_wet);
-//  - sqrt.approx.f32 (within about 1 ulp; no denormal flushing);
+//  - division as div.approx.ftz (the numerator times rcp.approx, within 2 ulp while the denominator's magnitude lies
+//    in [2^-126, 2^126]: every denominator of the face pass is a depth, area, width, cell size or clamp of them,
+//    bounded below by 1e-30 or by e_wet);
+//  - sqrt.approx.ftz (within about 1 ulp);
 //  - the cube root of x >= 0 from the hardware log2 and exp2 estimates (within about 2^-18 relative) refined by one
 //    Newton step, y - (y^3 - x) / (3 y^2), which squares that error away: within a few ulp. x = 0, and x so small that
 //    the estimate is 0, give 0.
+// The .ftz forms take a subnormal operand or result as zero, so they need no rescaling around the hardware estimate:
+// a quotient or root that would have been subnormal (below 2^-126, about 1.2e-38) reads as 0, an absolute change
+// smaller than that.
+__device__ __forceinline__ float div_approx(float a, float b) {
+    float y;
+    asm("div.approx.ftz.f32 %0, %1, %2;" : "=f"(y) : "f"(a), "f"(b));
+    return y;
+}
 __device__ __forceinline__ float sqrt_approx(float x) {
     float y;
-    asm("sqrt.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
 __device__ __forceinline__ float cbrt_fast(float x) {
@@ -278,7 +286,7 @@ __device__ __forceinline__ float fmax32(float a, float b) { return a >= b ? a : 
 __device__ __forceinline__ float fmin32(float a, float b) { return a <= b ? a : b; }
 
 #ifdef W2B_FAST
-__device__ __forceinline__ float qdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ float qdiv(float a, float b) { return div_approx(a, b); }
 __device__ __forceinline__ float qsqrt(float x) { return sqrt_approx(x); }
 __device__ __forceinline__ float qcbrt(float x) { return cbrt_fast(x); }
 // the hardware max and min, one instruction each: the same as fmax32 / fmin32 for ordered operands but for the sign of

@@ -247,7 +247,7 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int sl, int loc
         return mst ? sm[L::M + AX * L::S + sl] : __fmul_rn(HALF * (HO[b - S] + HO[b]) * dx, uf);
     };
 #ifdef W2B_FAST
-    const float rspan = __fdividef(ONE, span);
+    const float rspan = rcp_approx(span);
     const float press = dt * P.g * d_eta * rspan;
     float us;
     if (abar > 1e-6f * dx)
@@ -280,7 +280,7 @@ __device__ __forceinline__ float face_bc(const float* sm, int b, int sl, int loc
         const float e0 = rowc[2 * r] * top;
         const float de = rowc[2 * r + 1] * top;
 #ifdef W2B_FAST
-        const float rde = __fdividef(ONE, de);  // one reciprocal for both quotients
+        const float rde = rcp_approx(de);  // one reciprocal for both quotients
         const float f = (e - e0) * rde;
         area = q.x + f * (q.z - q.x);
         tt = q.y + f * (q.w - q.y);

@@ -1046,21 +1046,41 @@ __device__ __forceinline__ void envelope_cell(const StepArgs& A, int fid, int k,
 // The envelope after a step of the device loop, for the own cells of the work list's tiles whose runs record it at
 // this step (F_MAX); boundary cells are recorded by the boundary pass after its overwrite. A CTA a tile at a time, a
 // thread a cell; on steps that record no envelope every CTA returns at once.
+// A tile's place (work list -> tile -> its run, its first own cell, its rows' boundary marks) is a chain of dependent
+// loads, each from L2; the CTA stages it for ENV_CHUNK of its tiles at once in shared memory (all chains in flight
+// together), so that a tile's own work waits on its run's flags (L1-resident) and then on its cells' data only.
+constexpr int ENV_CHUNK = 64;
 __global__ void __launch_bounds__(TILE2, 2) envelope_kernel(StepArgs A) {
+    __shared__ int3 place[ENV_CHUNK];            // tile, run, native index of the tile's first own cell
+    __shared__ uint32_t marks[ENV_CHUNK * TILE];  // the tile's boundary marks, a word a row
     Ctl* ctl = A.ctl;
     if (!(ctl->any & ANY_MAX)) return;
     const int nwork = ctl->nwork;
     const float arrive = ctl->arrive, deep = ctl->deep;
     const int tid = threadIdx.x, jj = tid >> 5, ii = tid & 31;
-    for (int a = blockIdx.x; a < nwork; a += gridDim.x) {
-        const int t = A.list[a];
-        const int run = A.tile_run[t];
-        if ((A.R.flags[run] & (F_RUN | F_MAX)) != (F_RUN | F_MAX)) continue;
-        if ((A.bmark[t * TILE + jj] >> ii) & 1u) continue;
-        const int p = A.R.parity[run];
-        const int k = (A.tiles[2 * t] * TILE + GY + jj) * A.px + A.tiles[2 * t + 1] * TILE + GX + ii;
-        envelope_cell(A, t * TILE2 + tid, k, A.d[k], A.hh[1 - p][k], A.R.max_time[run], arrive, deep, A.uu[0][1 - p],
-                      A.uu[1][1 - p]);
+    const int G = gridDim.x;
+    const int mine = (nwork - (int)blockIdx.x + G - 1) / G;  // this CTA's tiles: work positions blockIdx.x + i G
+    for (int c0 = 0; c0 < mine; c0 += ENV_CHUNK) {
+        const int nc = min(ENV_CHUNK, mine - c0);
+        if (tid < nc) {
+            const int t = A.list[blockIdx.x + (c0 + tid) * G];
+            place[tid] = make_int3(t, A.tile_run[t],
+                                   (A.tiles[2 * t] * TILE + GY) * A.px + A.tiles[2 * t + 1] * TILE + GX);
+        }
+        __syncthreads();
+        for (int q = tid; q < nc * TILE; q += TILE2) marks[q] = A.bmark[place[q / TILE].x * TILE + q % TILE];
+        __syncthreads();
+        for (int i = 0; i < nc; ++i) {
+            const int3 w = place[i];
+            const int run = w.y;
+            if ((A.R.flags[run] & (F_RUN | F_MAX)) != (F_RUN | F_MAX)) continue;
+            if ((marks[i * TILE + jj] >> ii) & 1u) continue;
+            const int p = A.R.parity[run];
+            const int k = w.z + jj * A.px + ii;
+            envelope_cell(A, w.x * TILE2 + tid, k, A.d[k], A.hh[1 - p][k], A.R.max_time[run], arrive, deep,
+                          A.uu[0][1 - p], A.uu[1][1 - p]);
+        }
+        __syncthreads();  // the chunk's places and marks are read by every thread before the next chunk's overwrite
     }
 }
 

@@ -209,9 +209,10 @@ def cut_block(c, grid) -> None:
 
 def cpu_block(grid) -> tuple[int, int, int]:
     """First row and column (padded cells) and side of the CPU sample: a 32 x 32-tile block from the middle of the
-    grid."""
-    B = CPU_BLOCK_TILES
+    grid, smaller on a grid of fewer than 33 tiles a side (a tile short of its side, so that the block's pixels with
+    their rim lie inside the bed)."""
     nty, ntx = grid.tile_of.shape
+    B = max(1, min(CPU_BLOCK_TILES, nty - 1, ntx - 1))
     return (nty - B) // 2 * 32, (ntx - B) // 2 * 32, B * 32
 
 
@@ -341,7 +342,8 @@ def run_reference(args) -> None:
     del c.z
     block = block_inputs(c, grid, peak_rate(c))
     value, done, el, cells = cpu_sample(block, 0.0, threads, steps=args.steps, warmup=args.warmup)
-    sample = f"{CPU_BLOCK_TILES}x{CPU_BLOCK_TILES} tiles ({cells} cells) of the workload, {done} steps"
+    B = cpu_block(grid)[2] // 32
+    sample = f"{B}x{B} tiles ({cells} cells) of the workload, {done} steps"
     line = {
         "impl": "reference", "metric": "cell-steps/s", "value": value, "unit": "cell-steps/s", "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / max(done, 1),
@@ -1010,9 +1012,9 @@ def main() -> None:
         if args.parity_steps > 0:
             parity = block_parity(block, args.arith, args.parity_steps, threads)
         cv, done, el, ccells = cpu_sample(block, args.cpu_seconds, threads)
+        B = cpu_block(grid)[2] // 32
         cpu = {"value": cv, "unit": "cell-steps/s", "cores": threads, "kind": "port",
-               "sample": f"{CPU_BLOCK_TILES}x{CPU_BLOCK_TILES} tiles ({ccells} cells) of the workload, {done} steps "
-                         f"in {el:.1f} s"}  # fmt: skip
+               "sample": f"{B}x{B} tiles ({ccells} cells) of the workload, {done} steps in {el:.1f} s"}  # fmt: skip
     sweep = None
     if rank == 0 and world == 1 and not args.no_sweep:
         # the other half of the metric, bounded: the critical-duration storm sweep at 128 x 128 cells, 100 candidates

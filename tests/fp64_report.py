@@ -1,6 +1,6 @@
 """The CUDA path's error against the FP64 run, field by field, as configuration 1 (256 x 256 cells) steps on: one
-JSON line per step count, then the crest case's line (test infrastructure; run on a GPU box from the repository
-root: ``python tests/fp64_report.py``)."""
+JSON line per step count, then the crest case's line (test infrastructure; run on a machine with a B200, from the
+repository root: ``python tests/fp64_report.py``)."""
 
 from __future__ import annotations
 

@@ -1,5 +1,5 @@
-"""The exact-solution cases of tests/test_gpu_validation.py with their numbers (test infrastructure; run on a GPU box
-from the repository root: ``python tests/validation_report.py``): one JSON line a case."""
+"""The exact-solution cases of tests/test_gpu_validation.py with their numbers (test infrastructure; run on a machine
+with a B200, from the repository root: ``python tests/validation_report.py``): one JSON line a case."""
 
 from __future__ import annotations
 

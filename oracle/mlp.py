@@ -1,5 +1,5 @@
-"""Test infrastructure: the CPU oracle of the surrogate network (wadi2d_b200/surrogate.py). It is the checker for the
-device's forward pass and gradients, never the implementation. The surrogate has no counterpart in the reference
+"""Test infrastructure: the CPU oracle of the surrogate network (wadi2d_b200/surrogate.py). The tests compare the
+device's forward pass and gradients with it; it is never the implementation. The surrogate has no counterpart in the reference
 (its critical-duration search and network are new pieces), so this oracle restates the network's definition in
 FP64 and rounds to BF16 at the same points as the device: the weights' copies, the inputs, the activations between
 layers and the gradients w.r.t. the pre-activations (round to nearest even, as __float2bfloat16_rn). The two then

@@ -1,7 +1,7 @@
 """Test infrastructure: the CPU oracle of the surrogate network (wadi2d_b200/surrogate.py). The tests compare the
-device's forward pass and gradients with it; it is never the implementation. The surrogate has no counterpart in the reference
-(its critical-duration search and network are new pieces), so this oracle restates the network's definition in
-FP64 and rounds to BF16 at the same points as the device: the weights' copies, the inputs, the activations between
+device's forward pass and gradients with it; it is never the implementation. The surrogate has no counterpart in the
+reference (its critical-duration search and network are new pieces), so this oracle restates the network's definition
+in FP64 and rounds to BF16 at the same points as the device: the weights' copies, the inputs, the activations between
 layers and the gradients w.r.t. the pre-activations (round to nearest even, as __float2bfloat16_rn). The two then
 differ only by the accumulation order of FP32 against FP64 sums (and the rare BF16 rounding that the difference
 tips)."""
